@@ -1,0 +1,232 @@
+/*
+ * magritte_b200.h -- C ABI of the B200 radiation hot path.
+ *
+ * One opaque handle owns one model resident on one GPU.  Every entry point
+ * returns an mgr_status (0 = success); mgr_last_error() gives the message of
+ * the last failure on a handle.  No entry point aborts, asserts or traps:
+ * device-side failures (a ray that cannot be traced, a singular rate matrix)
+ * are counted on the device and reported as status codes.
+ *
+ * Each entry point names the Magritte member it replaces (paths inside the
+ * UCL/Magritte source tree).  The reference's Simulation is single-threaded
+ * at its interface; so is a handle (one host thread and one CUDA stream per
+ * handle).
+ */
+#ifndef MAGRITTE_B200_H
+#define MAGRITTE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MGR_OK = 0,
+    MGR_ERR_INVALID_ARG = 1,   /* bad pointer, size or order of calls        */
+    MGR_ERR_TRACE = 2,         /* a ray found no neighbour ahead of it       */
+    MGR_ERR_LU_SINGULAR = 3,   /* a cell's rate matrix had a zero pivot      */
+    MGR_ERR_NOT_CONVERGED = 4, /* ALI stopped at max_iter                    */
+    MGR_ERR_CUDA = 5,          /* a CUDA runtime call failed                 */
+    MGR_ERR_TIMEOUT = 6,       /* a bounded device wait ran out              */
+    MGR_ERR_UNSUPPORTED = 7,   /* input outside what the device path covers  */
+    MGR_ERR_STATE = 8,         /* called before the step it depends on       */
+    MGR_ERR_NO_MEMORY = 9      /* a device allocation failed                 */
+} mgr_status;
+
+typedef enum {
+    MGR_FP64 = 0,   /* every step in double precision                        */
+    MGR_MIXED = 1   /* opacities, source functions and optical depths in
+                       float, Feautrier elimination and rate equations in
+                       double                                                */
+} mgr_precision;
+
+/* One collision partner of the line species
+ * (Lines/LineProducingSpecies/Linedata/CollisionPartner/collisionPartner.hpp). */
+typedef struct {
+    int32_t ntmp;              /* temperatures in the rate table            */
+    int32_t ncol;              /* collisional transitions                   */
+    int32_t ortho_para;        /* 0 'n', 1 ortho-H2 ('o'), 2 para-H2 ('p')  */
+    int32_t reserved;
+    const int64_t *icol;       /* [ncol] upper level                        */
+    const int64_t *jcol;       /* [ncol] lower level                        */
+    const double  *tmp;        /* [ntmp] K, ascending                       */
+    const double  *Cd;         /* [ntmp*ncol] downward rates, m^3 s^-1      */
+    const double  *Ce;         /* [ntmp*ncol] upward rates, m^3 s^-1        */
+    const double  *abundance;  /* [ncells] partner number density, m^-3     */
+} mgr_colpar_desc;
+
+/* The model as Magritte's Model holds it (Model/model.hpp:23-44), with one
+ * line-producing species.  Host pointers; mgr_upload_model copies them. */
+typedef struct {
+    int64_t ncells;
+    const double  *position;       /* [ncells*3] m                          */
+    const double  *velocity;       /* [ncells*3] fraction of c              */
+    const int64_t *nbr_offsets;    /* [ncells+1] CSR offsets                */
+    const int64_t *nbr_list;       /* neighbour cells, in list order        */
+    int64_t nboundary;
+    const int64_t *boundary2cell;  /* [nboundary]                           */
+    const double  *boundary_temperature; /* [nboundary] K, NULL: T_CMB      */
+    int64_t nrays;
+    const double  *rays;           /* [nrays*3] unit vectors                */
+    const double  *ray_weights;    /* [nrays]                               */
+    const double  *temperature;    /* [ncells] K                            */
+    const double  *vturb2;         /* [ncells] (v_turb/c)^2                 */
+    int32_t nlev;
+    int32_t nrad;
+    const double  *energy;         /* [nlev] J                              */
+    const double  *weight;         /* [nlev] statistical weights            */
+    const int64_t *irad;           /* [nrad] upper level of each line       */
+    const int64_t *jrad;           /* [nrad] lower level                    */
+    const double  *A;              /* [nrad] s^-1                           */
+    const double  *Bs;             /* [nrad] stimulated emission            */
+    const double  *Ba;             /* [nrad] absorption                     */
+    const double  *frequency;      /* [nrad] Hz                             */
+    double inverse_mass;           /* 1 / (mass in amu)                     */
+    const double  *population_tot; /* [ncells] m^-3                         */
+    int32_t nquads;
+    int32_t ncolpar;
+    const double  *quad_roots;     /* [nquads] ascending, Doppler widths    */
+    const double  *quad_weights;   /* [nquads]                              */
+    const mgr_colpar_desc *colpar; /* [ncolpar]                             */
+    double pop_prec;               /* Parameters::pop_prec                  */
+    double max_width_fraction;     /* Parameters::max_width_fraction (0.5)  */
+} mgr_model_desc;
+
+/* Options of the ALI loop.  Replaces the arguments of
+ * Simulation::compute_level_populations(io, use_Ng, max_niterations). */
+typedef struct {
+    int32_t use_ng;        /* Ng acceleration every 5th iteration          */
+    int32_t precision;     /* mgr_precision                                */
+    int64_t max_iter;      /* 1000 in the reference's default overload     */
+    double  tol_max_rel;   /* > 0: stop once max over (cell, level) of
+                              2|n - n_prev|/(n + n_prev) < tol (levels with
+                              n > 1e-10 n_tot); <= 0: the reference's stop
+                              test, fraction_not_converged <= 0.005        */
+    int32_t use_graph;     /* replay each iteration as a CUDA graph        */
+    int32_t reserved;
+} mgr_ali_opts;
+
+typedef struct mgr_handle mgr_handle;
+
+/* --- lifetime ----------------------------------------------------------- */
+
+/* New handle on CUDA device `device`.  Replaces constructing Simulation
+ * (Simulation/simulation.hpp:49-166). */
+mgr_status mgr_create(int device, mgr_handle **out);
+
+/* Frees every device buffer of the handle. */
+mgr_status mgr_destroy(mgr_handle *h);
+
+/* Message of the last failed call on h (never NULL). */
+const char *mgr_last_error(const mgr_handle *h);
+
+/* Library version string. */
+const char *mgr_version(void);
+
+/* Copies the model to the device and derives antipodal rays
+ * (Rays::setup_antipodal_rays, Model/Geometry/Rays/rays.cpp:90-102) and the
+ * boundary maps.  Replaces Simulation::read (Model/model.cpp). */
+mgr_status mgr_upload_model(mgr_handle *h, const mgr_model_desc *model);
+
+/* Caps device memory used for stored ray traces (bytes; 0 = automatic).
+ * Beyond it, traces are recomputed per batch of origins each solve. */
+mgr_status mgr_set_trace_budget(mgr_handle *h, int64_t bytes);
+
+/* --- set-up steps (Simulation/simulation.hpp) --------------------------- */
+
+/* Per-cell frequency grids nu = line + width*root.  The device path needs
+ * each cell's grid to be already ascending (lines apart by more than their
+ * quadrature span), i.e. the reference's heapsort to be the identity;
+ * otherwise MGR_ERR_UNSUPPORTED.  Replaces
+ * Simulation::compute_spectral_discretisation (Simulation/sim_spectrum.tpp:13-196). */
+mgr_status mgr_compute_spectral_discretisation(mgr_handle *h);
+
+/* Boundary intensities: Planck at each boundary cell's temperature
+ * (the model's, or T_CMB).  Replaces Simulation::compute_boundary_intensities
+ * (Simulation/sim_radiation.tpp:17-48). */
+mgr_status mgr_compute_boundary_intensities(mgr_handle *h);
+
+/* Boltzmann populations scaled to n_tot, then emissivities and opacities.
+ * Replaces Simulation::compute_LTE_level_populations
+ * (Simulation/sim_lines.tpp:10-16). */
+mgr_status mgr_compute_LTE_level_populations(mgr_handle *h);
+
+/* --- geometry ----------------------------------------------------------- */
+
+/* Traces every ray of every origin on the device (bit-exact with
+ * Geometry::trace_ray<CoMoving>, Model/Geometry/geometry.tpp:21-207) and
+ * keeps the traces while they fit the trace budget. */
+mgr_status mgr_trace(mgr_handle *h);
+
+/* npoints[r*ncells + o] = n_ar + n_r + 1 for r < nrays/2.  Replaces
+ * Simulation::get_npoints_on_rays<CoMoving> (Simulation/simulation.tpp:540-552). */
+mgr_status mgr_get_npoints_on_rays(mgr_handle *h, int64_t *npoints);
+
+/* Points of the trace of (origin o, ray r): cell numbers, Doppler shifts and
+ * distance increments (ProjectedCellData, Model/Geometry/raydata.hpp:17-35).
+ * *n receives the length; at most cap entries are written. */
+mgr_status mgr_get_trace(mgr_handle *h, int64_t o, int64_t r, int64_t cap,
+                         int64_t *cell, double *shift, double *dZ, int64_t *n);
+
+/* --- radiation field ---------------------------------------------------- */
+
+/* Formal solve over all ray pairs and frequencies: J (when kept), the line
+ * integrals Jlin and the diagonal ALO.  Replaces
+ * Simulation::compute_radiation_field (Simulation/sim_radiation.tpp:56-338). */
+mgr_status mgr_compute_radiation_field(mgr_handle *h, int32_t precision);
+
+/* Keep (1) or skip (0) the full J[ncells*nfreqs] in device memory; Jlin and
+ * the ALO are always produced.  Off by default. */
+mgr_status mgr_set_keep_J(mgr_handle *h, int32_t keep);
+
+/* --- level populations -------------------------------------------------- */
+
+/* Jeff = Jlin - (h/4 pi) Ls n_i.  Replaces Simulation::compute_Jeff
+ * (Simulation/sim_lines.tpp:176-220). */
+mgr_status mgr_compute_Jeff(mgr_handle *h);
+
+/* Statistical equilibrium per cell, convergence statistics, emissivities and
+ * opacities.  Replaces Simulation::compute_level_populations_from_stateq
+ * (Simulation/sim_lines.tpp:24-30 -> lineProducingSpecies.tpp:120-171, 249-495). */
+mgr_status mgr_compute_level_populations_from_stateq(mgr_handle *h);
+
+/* One Ng-accelerated step, convergence statistics, emissivities and
+ * opacities.  Replaces Lines::iteration_using_Ng_acceleration
+ * (Model/Lines/lines.cpp:131-149). */
+mgr_status mgr_ng_acceleration(mgr_handle *h);
+
+/* fraction_not_converged, relative_change_mean and the max relative change
+ * of the last population update (lineProducingSpecies.tpp:120-171). */
+mgr_status mgr_get_convergence(mgr_handle *h, double *fnc, double *rcm, double *max_rel);
+
+/* The full ALI loop.  *iterations receives the count, as the reference's
+ * return value; err_max_hist (optional, max_iter entries) the max relative
+ * change of every iteration.  Returns MGR_ERR_NOT_CONVERGED when max_iter is
+ * reached.  Replaces Simulation::compute_level_populations
+ * (Simulation/sim_lines.tpp:42-164). */
+mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts,
+                                         int64_t *iterations, double *err_max_hist);
+
+/* --- data movement ------------------------------------------------------ */
+
+mgr_status mgr_set_populations(mgr_handle *h, const double *pop);     /* [ncells*nlev] */
+mgr_status mgr_get_populations(mgr_handle *h, double *pop);           /* [ncells*nlev] */
+mgr_status mgr_get_J(mgr_handle *h, double *J);                       /* [ncells*nfreqs] */
+mgr_status mgr_get_Jlin(mgr_handle *h, double *Jlin);                 /* [ncells*nrad] */
+mgr_status mgr_get_Jeff(mgr_handle *h, double *Jeff);                 /* [ncells*nrad] */
+mgr_status mgr_get_lambda(mgr_handle *h, double *Ls);                 /* [ncells*nrad] */
+mgr_status mgr_get_emissivity_opacity(mgr_handle *h, double *eta, double *chi); /* [ncells*nrad] */
+mgr_status mgr_get_frequencies(mgr_handle *h, double *nu);            /* [ncells*nfreqs] */
+
+/* Device time of the last formal solve (ms, CUDA events on the handle's
+ * stream) and the ray-point-frequency updates it did. */
+mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates);
+
+/* Synchronises the handle's stream. */
+mgr_status mgr_synchronize(mgr_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

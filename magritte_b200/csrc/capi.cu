@@ -1,0 +1,903 @@
+// capi.cu -- the handle, device memory and the extern "C" entry points.
+//
+// A handle owns one model on one GPU.  Host code here validates inputs,
+// derives the small per-model tables (antipodal rays, profile widths, line
+// windows) with separately rounded double arithmetic, moves data, and runs
+// the kernels of trace.cu, solve.cu and levels.cu on the handle's stream.
+// C++ exceptions are used internally and never cross the C boundary.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <stdexcept>
+
+#include "mgr_internal.cuh"
+
+using namespace mgr;
+
+namespace {
+
+struct Failure {
+    mgr_status code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(mgr_status c, const std::string &m) { throw Failure{c, m}; }
+
+void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        if (e == cudaErrorMemoryAllocation) fail(MGR_ERR_NO_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+        fail(MGR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+__global__ void widen_kernel(const int32_t *in, int64_t *out, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+
+}  // namespace
+
+struct mgr_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+
+    // sizes
+    int64_t N = 0;
+    int nrays = 0, npairs = 0, nlev = 0, nrad = 0, nquads = 0, nfreqs = 0, ncolpar = 0;
+
+    std::vector<void *> model_allocs;
+    ModelView mv{};
+
+    // state
+    double *pop = nullptr, *prev1 = nullptr, *prev2 = nullptr, *prev3 = nullptr;
+    double *eps = nullptr, *kap = nullptr, *Jlin = nullptr, *Lam = nullptr, *Jeff = nullptr;
+    double *J = nullptr, *partials = nullptr, *stats = nullptr;
+    float2 *ek = nullptr;
+    DevFlags *flags = nullptr;
+    double *h_stats = nullptr;
+    DevFlags *h_flags = nullptr;
+    double mixed_scale = 1.0;
+
+    // traces
+    int32_t *len_all = nullptr;        // [nrays*N]
+    int64_t *off_all = nullptr;        // [nrays*N] when stored
+    int32_t *tcell = nullptr;
+    double *tshift = nullptr, *tdz = nullptr;
+    int64_t tcap = 0;                  // point capacity of tcell/tshift/tdz
+    int32_t *blen = nullptr;           // batch lengths [nrays*bcap]
+    int64_t *boff = nullptr;           // batch offsets
+    int64_t bcap = 0;                  // origins per batch capacity
+    void *scan_tmp = nullptr;
+    size_t scan_tmp_bytes = 0;
+    bool traced = false, stored = false;
+    int64_t total_points = 0;
+    int64_t batch_origins = 0;
+    int64_t trace_budget = 0;
+    double updates_per_solve = 0.0;
+    std::vector<int32_t> h_len;        // [nrays*N] host copy for npoints
+
+    bool model_loaded = false, line_set = false, bdy_set = false, pops_valid = false;
+    bool keep_J = false;
+    double last_solve_ms = 0.0, last_updates = 0.0;
+
+    std::vector<int64_t> antipod;
+};
+
+namespace {
+
+template <class T>
+T *dalloc(mgr_handle *h, int64_t count, std::vector<void *> *track) {
+    if (count <= 0) count = 1;
+    void *p = nullptr;
+    ck(cudaMalloc(&p, (size_t)count * sizeof(T)), "cudaMalloc");
+    if (track) track->push_back(p);
+    return (T *)p;
+}
+
+template <class T>
+T *upload(mgr_handle *h, const T *src, int64_t count, std::vector<void *> *track) {
+    T *d = dalloc<T>(h, count, track);
+    if (count > 0) ck(cudaMemcpy(d, src, (size_t)count * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    return d;
+}
+
+void free_ptr(void *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+void free_traces(mgr_handle *h) {
+    free_ptr((void *&)h->off_all);
+    free_ptr((void *&)h->tcell);
+    free_ptr((void *&)h->tshift);
+    free_ptr((void *&)h->tdz);
+    free_ptr((void *&)h->blen);
+    free_ptr((void *&)h->boff);
+    free_ptr(h->scan_tmp);
+    h->scan_tmp_bytes = 0;
+    h->tcap = 0;
+    h->bcap = 0;
+    h->traced = false;
+    h->stored = false;
+}
+
+void free_model(mgr_handle *h) {
+    free_traces(h);
+    free_ptr((void *&)h->len_all);
+    for (void *p : h->model_allocs) cudaFree(p);
+    h->model_allocs.clear();
+    void **state[] = {(void **)&h->pop, (void **)&h->prev1, (void **)&h->prev2, (void **)&h->prev3,
+                      (void **)&h->eps, (void **)&h->kap, (void **)&h->Jlin, (void **)&h->Lam,
+                      (void **)&h->Jeff, (void **)&h->J, (void **)&h->partials, (void **)&h->stats,
+                      (void **)&h->ek, (void **)&h->flags};
+    for (void **p : state) free_ptr(*p);
+    h->model_loaded = h->line_set = h->bdy_set = h->pops_valid = false;
+}
+
+void set_device(mgr_handle *h) { ck(cudaSetDevice(h->device), "cudaSetDevice"); }
+
+void reset_flags(mgr_handle *h) {
+    ck(cudaMemsetAsync(h->flags, 0, sizeof(DevFlags), h->stream), "reset flags");
+}
+
+// Reads the device error counters; returns the status they imply.
+void check_flags(mgr_handle *h, const char *what) {
+    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream),
+       "read flags");
+    ck(cudaStreamSynchronize(h->stream), what);
+    const DevFlags &f = *h->h_flags;
+    if (f.trace_err || f.stuck_err)
+        fail(MGR_ERR_TRACE, std::string(what) + ": " + std::to_string(f.trace_err + f.stuck_err) +
+                                " ray(s) found no neighbour ahead before reaching a boundary cell");
+    if (f.interp_err)
+        fail(MGR_ERR_TRACE, std::string(what) + ": more than 10000 interpolation points needed on " +
+                                std::to_string(f.interp_err) + " ray step(s)");
+    if (f.cap_err) fail(MGR_ERR_CUDA, std::string(what) + ": trace slot overflow (internal)");
+    if (f.lu_err)
+        fail(MGR_ERR_LU_SINGULAR, std::string(what) + ": zero pivot in the rate equations of " +
+                                      std::to_string(f.lu_err) + " cell(s)");
+}
+
+LevelArgs level_args(mgr_handle *h) {
+    LevelArgs a{};
+    a.pop = h->pop; a.prev1 = h->prev1; a.prev2 = h->prev2; a.prev3 = h->prev3;
+    a.eps = h->eps; a.kap = h->kap; a.ehat_khat = h->ek; a.mixed_scale = h->mixed_scale;
+    a.Jlin = h->Jlin; a.Lam = h->Lam; a.Jeff = h->Jeff;
+    a.partials = h->partials; a.stats = h->stats;
+    a.npartials = level_partials_needed(h->mv);
+    return a;
+}
+
+void need(bool ok, mgr_status c, const char *msg) {
+    if (!ok) fail(c, msg);
+}
+
+// Profile width over c, Thermodynamics::profile_width (thermodynamics.tpp:62-69).
+// Separately rounded (this file is compiled with -ffp-contract=off).
+double profile_width_host(double inverse_mass, double T, double vturb2) {
+    volatile double a = kTWO_KB_OVER_AMU_C_SQUARED * inverse_mass;
+    volatile double b = a * T;
+    volatile double c = b + vturb2;
+    return std::sqrt((double)c);
+}
+
+// ------------------------------------------------------------------ upload
+void do_upload(mgr_handle *h, const mgr_model_desc *d) {
+    need(d != nullptr, MGR_ERR_INVALID_ARG, "model descriptor is NULL");
+    need(d->ncells > 0 && d->ncells < (int64_t)INT32_MAX, MGR_ERR_INVALID_ARG, "ncells out of range");
+    need(d->position && d->velocity && d->nbr_offsets && d->nbr_list && d->boundary2cell &&
+             d->rays && d->ray_weights && d->temperature && d->vturb2 && d->energy && d->weight &&
+             d->irad && d->jrad && d->A && d->Bs && d->Ba && d->frequency && d->population_tot &&
+             d->quad_roots && d->quad_weights,
+         MGR_ERR_INVALID_ARG, "a required model array is NULL");
+    need(d->nlev >= 2 && d->nlev <= kMaxLevels, MGR_ERR_UNSUPPORTED, "nlev must be in [2, 32]");
+    need(d->nrad >= 1, MGR_ERR_INVALID_ARG, "nrad must be >= 1");
+    need(d->nquads >= 1, MGR_ERR_INVALID_ARG, "nquads must be >= 1");
+    need(d->nrays >= 2 && d->nrays % 2 == 0, MGR_ERR_INVALID_ARG, "nrays must be even and >= 2");
+    need(d->ncolpar >= 0 && d->ncolpar <= kMaxColpar, MGR_ERR_UNSUPPORTED, "at most 4 collision partners");
+    need(d->ncolpar == 0 || d->colpar, MGR_ERR_INVALID_ARG, "colpar is NULL");
+    need(d->nboundary >= 1, MGR_ERR_INVALID_ARG, "nboundary must be >= 1");
+    need((int64_t)d->nrad * d->nquads < (int64_t)INT32_MAX, MGR_ERR_INVALID_ARG, "too many bins");
+
+    free_model(h);
+    set_device(h);
+    const int64_t N = d->ncells;
+    h->N = N;
+    h->nrays = (int)d->nrays;
+    h->npairs = (int)(d->nrays / 2);
+    h->nlev = d->nlev;
+    h->nrad = d->nrad;
+    h->nquads = d->nquads;
+    h->nfreqs = d->nrad * d->nquads;
+    h->ncolpar = d->ncolpar;
+    auto *T = &h->model_allocs;
+
+    // neighbours (int32 on the device)
+    const int64_t nnb = d->nbr_offsets[N];
+    need(d->nbr_offsets[0] == 0 && nnb >= 0 && nnb < (int64_t)INT32_MAX, MGR_ERR_INVALID_ARG,
+         "neighbour offsets out of range");
+    std::vector<int32_t> off32(N + 1), nb32(std::max<int64_t>(nnb, 1));
+    for (int64_t p = 0; p <= N; p++) {
+        if (p < N) need(d->nbr_offsets[p + 1] >= d->nbr_offsets[p], MGR_ERR_INVALID_ARG, "neighbour offsets not ascending");
+        off32[p] = (int32_t)d->nbr_offsets[p];
+    }
+    for (int64_t k = 0; k < nnb; k++) {
+        need(d->nbr_list[k] >= 0 && d->nbr_list[k] < N, MGR_ERR_INVALID_ARG, "neighbour index out of range");
+        nb32[k] = (int32_t)d->nbr_list[k];
+    }
+
+    // boundary
+    std::vector<uint8_t> bmask(N, 0);
+    std::vector<int32_t> c2b(N, -1);
+    for (int64_t b = 0; b < d->nboundary; b++) {
+        const int64_t c = d->boundary2cell[b];
+        need(c >= 0 && c < N, MGR_ERR_INVALID_ARG, "boundary cell out of range");
+        bmask[c] = 1;
+        c2b[c] = (int32_t)b;
+    }
+    std::vector<double> bT(d->nboundary, kT_CMB);
+    if (d->boundary_temperature)
+        for (int64_t b = 0; b < d->nboundary; b++) bT[b] = d->boundary_temperature[b];
+
+    // rays and antipodes (Rays::setup_antipodal_rays, rays.cpp:90-102)
+    h->antipod.assign(d->nrays, -1);
+    for (int64_t r1 = 0; r1 < d->nrays; r1++)
+        for (int64_t r2 = 0; r2 < d->nrays; r2++) {
+            const double *a = d->rays + 3 * r1, *b = d->rays + 3 * r2;
+            const double sx = a[0] + b[0], sy = a[1] + b[1], sz = a[2] + b[2];
+            if ((sx * sx + sy * sy) + sz * sz < 1.0E-9) h->antipod[r1] = r2;
+        }
+    std::vector<int32_t> ap32(d->nrays);
+    for (int64_t r = 0; r < d->nrays; r++) {
+        if (r < d->nrays / 2) need(h->antipod[r] >= 0, MGR_ERR_INVALID_ARG, "a ray of the first half has no antipode");
+        ap32[r] = (int32_t)h->antipod[r];
+    }
+
+    // thermodynamics
+    std::vector<double> pw(N), ipw(N), dsm(N);
+    double pw_max = 0.0, pw_min = std::numeric_limits<double>::max(), vmax = 0.0;
+    for (int64_t p = 0; p < N; p++) {
+        pw[p] = profile_width_host(d->inverse_mass, d->temperature[p], d->vturb2[p]);
+        need(pw[p] > 0.0 && std::isfinite(pw[p]), MGR_ERR_INVALID_ARG, "non-positive profile width");
+        ipw[p] = 1.0 / pw[p];
+        dsm[p] = d->max_width_fraction * pw[p];
+        pw_max = std::max(pw_max, pw[p]);
+        pw_min = std::min(pw_min, pw[p]);
+        const double *v = d->velocity + 3 * p;
+        vmax = std::max(vmax, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+    }
+
+    // lines: the device path keeps the transitions' order, which must be
+    // ascending in frequency (Lines::setup's heapsort then is the identity)
+    std::vector<double> line(d->nrad), iline(d->nrad);
+    for (int k = 0; k < d->nrad; k++) {
+        line[k] = d->frequency[k];
+        need(line[k] > 0.0, MGR_ERR_INVALID_ARG, "non-positive line frequency");
+        if (k) need(line[k] > line[k - 1], MGR_ERR_UNSUPPORTED, "line frequencies must be ascending");
+        iline[k] = 1.0 / line[k];
+        need(d->irad[k] >= 0 && d->irad[k] < d->nlev && d->jrad[k] >= 0 && d->jrad[k] < d->nlev,
+             MGR_ERR_INVALID_ARG, "irad/jrad out of range");
+    }
+    for (int z = 1; z < d->nquads; z++)
+        need(d->quad_roots[z] > d->quad_roots[z - 1], MGR_ERR_UNSUPPORTED, "quadrature roots must be ascending");
+
+    // conservative window of lines a bin can see (+-11 widths around any
+    // Doppler-shifted frequency of the bin)
+    std::vector<int32_t> wlo(d->nrad), whi(d->nrad);
+    {
+        const double sdev = 2.0 * vmax * (1.0 + 1e-9) + 1e-15;
+        const double rlo = std::min(d->quad_roots[0], 0.0), rhi = std::max(d->quad_roots[d->nquads - 1], 0.0);
+        for (int k = 0; k < d->nrad; k++) {
+            const double nlo = line[k] * (1.0 + pw_max * rlo) * (1.0 - sdev) * (1.0 - 1e-12);
+            const double nhi = line[k] * (1.0 + pw_max * rhi) * (1.0 + sdev) * (1.0 + 1e-12);
+            int lo = k, hi = k;
+            for (int l = 0; l < d->nrad; l++) {
+                const double wl = line[l] * (1.0 - 11.0 * pw_max) * (1.0 - 1e-12);
+                const double wh = line[l] * (1.0 + 11.0 * pw_max) * (1.0 + 1e-12);
+                if (nhi >= wl && nlo <= wh) { lo = std::min(lo, l); hi = std::max(hi, l); }
+            }
+            wlo[k] = lo;
+            whi[k] = hi;
+        }
+    }
+
+    // scale of the float opacities: a power of two that brings the largest
+    // possible line-centre opacity (over c) near one
+    {
+        double bamax = 0.0, ptmax = 0.0;
+        for (int k = 0; k < d->nrad; k++) bamax = std::max(bamax, std::fabs(d->Ba[k]));
+        for (int64_t p = 0; p < N; p++) ptmax = std::max(ptmax, d->population_tot[p]);
+        const double kest = kHH_OVER_FOUR_PI * ptmax * bamax * kINVERSE_SQRT_PI / pw_min;
+        int e = 0;
+        if (kest > 0.0 && std::isfinite(kest)) e = -(int)std::lround(std::log2(kest));
+        e = std::max(-100, std::min(120, e));
+        h->mixed_scale = std::ldexp(1.0, e);
+    }
+
+    // upload
+    ModelView &m = h->mv;
+    m = ModelView{};
+    m.N = N;
+    m.nrays = h->nrays;
+    m.npairs = h->npairs;
+    m.nlev = h->nlev;
+    m.nrad = h->nrad;
+    m.nquads = h->nquads;
+    m.nfreqs = h->nfreqs;
+    m.ncolpar = h->ncolpar;
+    m.pop_prec = d->pop_prec;
+    m.pos = upload(h, d->position, 3 * N, T);
+    m.vel = upload(h, d->velocity, 3 * N, T);
+    m.rays = upload(h, d->rays, 3 * (int64_t)d->nrays, T);
+    m.ray_w = upload(h, d->ray_weights, d->nrays, T);
+    m.nbr_off = upload(h, off32.data(), N + 1, T);
+    m.nbr = upload(h, nb32.data(), (int64_t)nb32.size(), T);
+    m.boundary = upload(h, bmask.data(), N, T);
+    m.cell2bdy = upload(h, c2b.data(), N, T);
+    m.antipod = upload(h, ap32.data(), d->nrays, T);
+    m.bdy_T = upload(h, bT.data(), d->nboundary, T);
+    m.T = upload(h, d->temperature, N, T);
+    m.dshift_max = upload(h, dsm.data(), N, T);
+    m.pw = upload(h, pw.data(), N, T);
+    m.inv_pw = upload(h, ipw.data(), N, T);
+    m.line = upload(h, line.data(), d->nrad, T);
+    m.inv_line = upload(h, iline.data(), d->nrad, T);
+    m.A = upload(h, d->A, d->nrad, T);
+    m.Bs = upload(h, d->Bs, d->nrad, T);
+    m.Ba = upload(h, d->Ba, d->nrad, T);
+    m.energy = upload(h, d->energy, d->nlev, T);
+    m.weight = upload(h, d->weight, d->nlev, T);
+    std::vector<int32_t> ir(d->nrad), jr(d->nrad);
+    for (int k = 0; k < d->nrad; k++) { ir[k] = (int32_t)d->irad[k]; jr[k] = (int32_t)d->jrad[k]; }
+    m.irad = upload(h, ir.data(), d->nrad, T);
+    m.jrad = upload(h, jr.data(), d->nrad, T);
+    m.win_lo = upload(h, wlo.data(), d->nrad, T);
+    m.win_hi = upload(h, whi.data(), d->nrad, T);
+    m.roots = upload(h, d->quad_roots, d->nquads, T);
+    m.qw = upload(h, d->quad_weights, d->nquads, T);
+    m.pop_tot = upload(h, d->population_tot, N, T);
+    for (int c = 0; c < d->ncolpar; c++) {
+        const mgr_colpar_desc &s = d->colpar[c];
+        need(s.ntmp >= 1 && s.ncol >= 0 && s.icol && s.jcol && s.tmp && s.Cd && s.Ce && s.abundance,
+             MGR_ERR_INVALID_ARG, "bad collision partner");
+        need(s.ortho_para >= 0 && s.ortho_para <= 2, MGR_ERR_INVALID_ARG, "bad ortho_para");
+        std::vector<int32_t> ic(std::max(1, s.ncol)), jc(std::max(1, s.ncol));
+        for (int k = 0; k < s.ncol; k++) {
+            need(s.icol[k] >= 0 && s.icol[k] < d->nlev && s.jcol[k] >= 0 && s.jcol[k] < d->nlev,
+                 MGR_ERR_INVALID_ARG, "icol/jcol out of range");
+            ic[k] = (int32_t)s.icol[k];
+            jc[k] = (int32_t)s.jcol[k];
+        }
+        ColparDev &cd = m.colpar[c];
+        cd.ntmp = s.ntmp;
+        cd.ncol = s.ncol;
+        cd.ortho_para = s.ortho_para;
+        cd.icol = upload(h, ic.data(), (int64_t)ic.size(), T);
+        cd.jcol = upload(h, jc.data(), (int64_t)jc.size(), T);
+        cd.tmp = upload(h, s.tmp, s.ntmp, T);
+        cd.Cd = upload(h, s.Cd, (int64_t)s.ntmp * s.ncol, T);
+        cd.Ce = upload(h, s.Ce, (int64_t)s.ntmp * s.ncol, T);
+        cd.abn = upload(h, s.abundance, N, T);
+    }
+
+    // state
+    const int64_t NL = N * h->nlev, NK = N * h->nrad;
+    h->pop = dalloc<double>(h, NL, nullptr);
+    h->prev1 = dalloc<double>(h, NL, nullptr);
+    h->prev2 = dalloc<double>(h, NL, nullptr);
+    h->prev3 = dalloc<double>(h, NL, nullptr);
+    h->eps = dalloc<double>(h, NK, nullptr);
+    h->kap = dalloc<double>(h, NK, nullptr);
+    h->ek = dalloc<float2>(h, NK, nullptr);
+    h->Jlin = dalloc<double>(h, NK, nullptr);
+    h->Lam = dalloc<double>(h, NK, nullptr);
+    h->Jeff = dalloc<double>(h, NK, nullptr);
+    h->partials = dalloc<double>(h, 5 * (int64_t)level_partials_needed(m), nullptr);
+    h->stats = dalloc<double>(h, 8, nullptr);
+    h->flags = dalloc<DevFlags>(h, 1, nullptr);
+    ck(cudaMemset(h->pop, 0, NL * sizeof(double)), "memset");
+    ck(cudaMemset(h->prev1, 0, NL * sizeof(double)), "memset");
+    ck(cudaMemset(h->prev2, 0, NL * sizeof(double)), "memset");
+    ck(cudaMemset(h->prev3, 0, NL * sizeof(double)), "memset");
+    ck(cudaMemset(h->Jlin, 0, NK * sizeof(double)), "memset");
+    ck(cudaMemset(h->Lam, 0, NK * sizeof(double)), "memset");
+    ck(cudaMemset(h->Jeff, 0, NK * sizeof(double)), "memset");
+    ck(cudaMemset(h->stats, 0, 8 * sizeof(double)), "memset");
+    ck(cudaMemset(h->flags, 0, sizeof(DevFlags)), "memset");
+    h->model_loaded = true;
+}
+
+// ------------------------------------------------------------------ traces
+void ensure_scan_tmp(mgr_handle *h, int64_t n) {
+    size_t bytes = 0;
+    ck(cub::DeviceScan::ExclusiveSum(nullptr, bytes, (int64_t *)nullptr, (int64_t *)nullptr, n, h->stream),
+       "scan size");
+    if (bytes > h->scan_tmp_bytes) {
+        free_ptr(h->scan_tmp);
+        ck(cudaMalloc(&h->scan_tmp, bytes), "cudaMalloc scan");
+        h->scan_tmp_bytes = bytes;
+    }
+}
+
+// Offsets of lens[0..n) (int32) into off (int64); returns the total.
+int64_t scan_lengths(mgr_handle *h, const int32_t *lens, int64_t *off, int64_t n) {
+    widen_kernel<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(lens, off, n);
+    ck(cudaGetLastError(), "widen");
+    ensure_scan_tmp(h, n);
+    size_t bytes = h->scan_tmp_bytes;
+    ck(cub::DeviceScan::ExclusiveSum(h->scan_tmp, bytes, off, off, n, h->stream), "scan");
+    int64_t last_off = 0;
+    int32_t last_len = 0;
+    ck(cudaMemcpyAsync(&last_off, off + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream), "d2h");
+    ck(cudaMemcpyAsync(&last_len, lens + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream), "d2h");
+    ck(cudaStreamSynchronize(h->stream), "scan sync");
+    return last_off + last_len;
+}
+
+void ensure_points(mgr_handle *h, int64_t npts) {
+    if (npts <= h->tcap) return;
+    free_ptr((void *&)h->tcell);
+    free_ptr((void *&)h->tshift);
+    free_ptr((void *&)h->tdz);
+    const int64_t cap = std::max<int64_t>(npts, 1);
+    h->tcell = dalloc<int32_t>(h, cap, nullptr);
+    h->tshift = dalloc<double>(h, cap, nullptr);
+    h->tdz = dalloc<double>(h, cap, nullptr);
+    h->tcap = cap;
+}
+
+constexpr int64_t kBytesPerPoint = sizeof(int32_t) + 2 * sizeof(double);
+
+int64_t default_budget(mgr_handle *h) {
+    size_t fr = 0, tot = 0;
+    ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+    return (int64_t)(0.6 * (double)fr);
+}
+
+void do_trace(mgr_handle *h) {
+    need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+    set_device(h);
+    free_traces(h);
+    const int64_t N = h->N, R = h->nrays, n = R * N;
+    if (!h->len_all) h->len_all = dalloc<int32_t>(h, n, nullptr);
+    reset_flags(h);
+    ck(launch_trace_count(h->mv, 0, N, h->len_all, h->flags, h->stream), "trace count");
+    check_flags(h, "trace");
+    h->h_len.resize(n);
+    ck(cudaMemcpy(h->h_len.data(), h->len_all, n * sizeof(int32_t), cudaMemcpyDeviceToHost), "d2h lens");
+    // ray-point-frequency updates of one formal solve
+    double U = 0.0;
+    int64_t total = 0;
+    std::vector<int64_t> per_origin(N, 0);
+    for (int64_t d = 0; d < R; d++)
+        for (int64_t o = 0; o < N; o++) {
+            total += h->h_len[d * N + o];
+            per_origin[o] += h->h_len[d * N + o];
+        }
+    for (int r = 0; r < h->npairs; r++) {
+        const int64_t ar = h->antipod[r];
+        for (int64_t o = 0; o < N; o++) {
+            const int64_t ndep = (int64_t)h->h_len[r * N + o] + h->h_len[ar * N + o] + 1;
+            if (ndep > 1) U += (double)ndep;
+        }
+    }
+    h->updates_per_solve = U * h->nfreqs;
+    h->total_points = total;
+    const int64_t budget = h->trace_budget > 0 ? h->trace_budget : default_budget(h);
+    if (total * kBytesPerPoint <= budget) {
+        h->off_all = dalloc<int64_t>(h, n, nullptr);
+        const int64_t tot = scan_lengths(h, h->len_all, h->off_all, n);
+        ensure_points(h, tot);
+        TraceView t{0, N, (int)R, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz};
+        reset_flags(h);
+        ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->flags, h->stream), "trace fill");
+        check_flags(h, "trace fill");
+        h->stored = true;
+        h->batch_origins = N;
+    } else {
+        // origins per batch so that the largest batch fits the budget
+        const int64_t cap_pts = std::max<int64_t>(budget / kBytesPerPoint, 1);
+        int64_t best = N;
+        for (;;) {
+            int64_t worst = 0;
+            for (int64_t o0 = 0; o0 < N; o0 += best) {
+                int64_t s = 0;
+                for (int64_t o = o0; o < std::min(N, o0 + best); o++) s += per_origin[o];
+                worst = std::max(worst, s);
+            }
+            if (worst <= cap_pts || best == 1) break;
+            best = std::max<int64_t>(1, best / 2);
+        }
+        h->batch_origins = best;
+        h->stored = false;
+    }
+    h->traced = true;
+}
+
+// Fills the trace store for origins [o0, o0+cnt) and returns its view.
+TraceView build_batch(mgr_handle *h, int64_t o0, int64_t cnt) {
+    const int64_t R = h->nrays;
+    if (cnt > h->bcap) {
+        free_ptr((void *&)h->blen);
+        free_ptr((void *&)h->boff);
+        h->blen = dalloc<int32_t>(h, R * cnt, nullptr);
+        h->boff = dalloc<int64_t>(h, R * cnt, nullptr);
+        h->bcap = cnt;
+    }
+    ck(cudaMemcpy2DAsync(h->blen, cnt * sizeof(int32_t), h->len_all + o0, h->N * sizeof(int32_t),
+                         cnt * sizeof(int32_t), R, cudaMemcpyDeviceToDevice, h->stream),
+       "batch lens");
+    const int64_t tot = scan_lengths(h, h->blen, h->boff, R * cnt);
+    ensure_points(h, tot);
+    TraceView t{o0, cnt, (int)R, h->boff, h->blen, h->tcell, h->tshift, h->tdz};
+    ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->flags, h->stream), "trace fill");
+    return t;
+}
+
+void do_solve(mgr_handle *h, int precision) {
+    need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
+    need(h->pops_valid, MGR_ERR_STATE, "no level populations yet (LTE or set_populations)");
+    need(precision == MGR_FP64 || precision == MGR_MIXED, MGR_ERR_INVALID_ARG, "bad precision");
+    set_device(h);
+    if (!h->traced) do_trace(h);
+    if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
+    SolveArgs a{};
+    a.eps = h->eps;
+    a.kap = h->kap;
+    a.ehat_khat = h->ek;
+    a.mixed_scale = h->mixed_scale;
+    a.Jlin = h->Jlin;
+    a.Lam = h->Lam;
+    a.J = h->keep_J ? h->J : nullptr;
+    reset_flags(h);
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
+    if (h->stored) {
+        TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz};
+        ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
+    } else {
+        for (int64_t o0 = 0; o0 < h->N; o0 += h->batch_origins) {
+            const int64_t cnt = std::min(h->batch_origins, h->N - o0);
+            TraceView t = build_batch(h, o0, cnt);
+            ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
+        }
+    }
+    ck(cudaEventRecord(h->ev1, h->stream), "event");
+    check_flags(h, "formal solve");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    h->last_solve_ms = ms;
+    h->last_updates = h->updates_per_solve;
+}
+
+void read_stats(mgr_handle *h) {
+    ck(cudaMemcpyAsync(h->h_stats, h->stats, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "stats");
+    ck(cudaStreamSynchronize(h->stream), "stats sync");
+}
+
+void do_stateq(mgr_handle *h) {
+    need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+    reset_flags(h);
+    ck(launch_stateq(h->mv, level_args(h), h->flags, h->stream), "stateq");
+    check_flags(h, "statistical equilibrium");
+    read_stats(h);
+}
+
+void do_ng(mgr_handle *h) {
+    need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+    const LevelArgs a = level_args(h);
+    ck(launch_ng(h->mv, a, h->stream), "ng");
+    ck(launch_convergence(h->mv, a, h->stream), "convergence");
+    ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
+    read_stats(h);
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+
+namespace {
+mgr_status run(mgr_handle *h, const std::function<void()> &fn) {
+    if (!h) return MGR_ERR_INVALID_ARG;
+    try {
+        fn();
+        h->err.clear();
+        return MGR_OK;
+    } catch (const Failure &f) {
+        h->err = f.msg;
+        return f.code;
+    } catch (const std::exception &e) {
+        h->err = e.what();
+        return MGR_ERR_INVALID_ARG;
+    } catch (...) {
+        h->err = "unknown error";
+        return MGR_ERR_INVALID_ARG;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char *mgr_version(void) { return "magritte_b200 0.1 (sm_100a)"; }
+
+mgr_status mgr_create(int device, mgr_handle **out) {
+    if (!out) return MGR_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return MGR_ERR_CUDA;
+    mgr_handle *h = new (std::nothrow) mgr_handle();
+    if (!h) return MGR_ERR_NO_MEMORY;
+    h->device = device;
+    const mgr_status s = run(h, [&] {
+        set_device(h);
+        ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+        ck(cudaEventCreate(&h->ev0), "event");
+        ck(cudaEventCreate(&h->ev1), "event");
+        ck(cudaMallocHost(&h->h_stats, 8 * sizeof(double)), "pinned");
+        ck(cudaMallocHost(&h->h_flags, sizeof(DevFlags)), "pinned");
+    });
+    if (s != MGR_OK) {
+        mgr_destroy(h);
+        return s;
+    }
+    *out = h;
+    return MGR_OK;
+}
+
+mgr_status mgr_destroy(mgr_handle *h) {
+    if (!h) return MGR_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_model(h);
+    if (h->h_stats) cudaFreeHost(h->h_stats);
+    if (h->h_flags) cudaFreeHost(h->h_flags);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MGR_OK;
+}
+
+const char *mgr_last_error(const mgr_handle *h) { return h ? h->err.c_str() : "NULL handle"; }
+
+mgr_status mgr_upload_model(mgr_handle *h, const mgr_model_desc *model) {
+    return run(h, [&] { do_upload(h, model); });
+}
+
+mgr_status mgr_set_trace_budget(mgr_handle *h, int64_t bytes) {
+    return run(h, [&] {
+        need(bytes >= 0, MGR_ERR_INVALID_ARG, "negative budget");
+        h->trace_budget = bytes;
+        free_traces(h);
+    });
+}
+
+mgr_status mgr_compute_spectral_discretisation(mgr_handle *h) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        // identity check of the reference's per-cell sort: within a line the
+        // roots ascend; consecutive lines must not interleave in any cell
+        std::vector<double> pw(h->N), line(h->nrad), roots(h->nquads);
+        ck(cudaMemcpy(pw.data(), h->mv.pw, h->N * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(line.data(), h->mv.line, h->nrad * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(roots.data(), h->mv.roots, h->nquads * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        for (int64_t p = 0; p < h->N; p++)
+            for (int k = 0; k + 1 < h->nrad; k++) {
+                volatile double w0 = line[k] * pw[p], w1 = line[k + 1] * pw[p];
+                volatile double a0 = w0 * roots[h->nquads - 1], a1 = w1 * roots[0];
+                const double top = line[k] + a0, bot = line[k + 1] + a1;
+                if (!(top < bot))
+                    fail(MGR_ERR_UNSUPPORTED,
+                         "line profiles interleave in cell " + std::to_string(p) +
+                             " (frequency grid not ascending); the device path needs separated lines");
+            }
+        h->line_set = true;
+    });
+}
+
+mgr_status mgr_compute_boundary_intensities(mgr_handle *h) {
+    return run(h, [&] {
+        need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
+        h->bdy_set = true;   // evaluated on the fly from the boundary temperatures
+    });
+}
+
+mgr_status mgr_compute_LTE_level_populations(mgr_handle *h) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        set_device(h);
+        const LevelArgs a = level_args(h);
+        ck(launch_lte(h->mv, a, h->stream), "lte");
+        ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
+        ck(cudaStreamSynchronize(h->stream), "lte sync");
+        h->pops_valid = true;
+    });
+}
+
+mgr_status mgr_trace(mgr_handle *h) {
+    return run(h, [&] { do_trace(h); });
+}
+
+mgr_status mgr_get_npoints_on_rays(mgr_handle *h, int64_t *npoints) {
+    return run(h, [&] {
+        need(npoints != nullptr, MGR_ERR_INVALID_ARG, "NULL output");
+        if (!h->traced) do_trace(h);
+        const int64_t N = h->N;
+        for (int r = 0; r < h->npairs; r++) {
+            const int64_t ar = h->antipod[r];
+            for (int64_t o = 0; o < N; o++)
+                npoints[r * N + o] = (int64_t)h->h_len[r * N + o] + h->h_len[ar * N + o] + 1;
+        }
+    });
+}
+
+mgr_status mgr_get_trace(mgr_handle *h, int64_t o, int64_t r, int64_t cap, int64_t *cell,
+                         double *shift, double *dZ, int64_t *n) {
+    return run(h, [&] {
+        need(n != nullptr, MGR_ERR_INVALID_ARG, "NULL n");
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        need(o >= 0 && o < h->N && r >= 0 && r < h->nrays, MGR_ERR_INVALID_ARG, "origin/ray out of range");
+        set_device(h);
+        if (!h->traced) do_trace(h);
+        const int64_t len = h->h_len[r * h->N + o];
+        *n = len;
+        const int64_t m = std::min(len, cap);
+        if (m <= 0) return;
+        need(cell && shift && dZ, MGR_ERR_INVALID_ARG, "NULL output arrays");
+        int64_t base = 0;
+        const int32_t *tc;
+        const double *ts, *tz;
+        if (h->stored) {
+            ck(cudaMemcpy(&base, h->off_all + r * h->N + o, sizeof(int64_t), cudaMemcpyDeviceToHost), "d2h");
+            tc = h->tcell; ts = h->tshift; tz = h->tdz;
+        } else {
+            TraceView t = build_batch(h, o, 1);
+            ck(cudaMemcpyAsync(&base, t.off + r, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream), "d2h");
+            ck(cudaStreamSynchronize(h->stream), "sync");
+            tc = h->tcell; ts = h->tshift; tz = h->tdz;
+        }
+        std::vector<int32_t> c(m);
+        ck(cudaMemcpy(c.data(), tc + base, m * sizeof(int32_t), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(shift, ts + base, m * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(dZ, tz + base, m * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        for (int64_t i = 0; i < m; i++) cell[i] = c[i];
+    });
+}
+
+mgr_status mgr_set_keep_J(mgr_handle *h, int32_t keep) {
+    return run(h, [&] { h->keep_J = keep != 0; });
+}
+
+mgr_status mgr_compute_radiation_field(mgr_handle *h, int32_t precision) {
+    return run(h, [&] { do_solve(h, precision); });
+}
+
+mgr_status mgr_compute_Jeff(mgr_handle *h) {
+    return run(h, [&] {
+        need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+        ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
+        ck(cudaStreamSynchronize(h->stream), "jeff sync");
+    });
+}
+
+mgr_status mgr_compute_level_populations_from_stateq(mgr_handle *h) {
+    return run(h, [&] { do_stateq(h); });
+}
+
+mgr_status mgr_ng_acceleration(mgr_handle *h) {
+    return run(h, [&] { do_ng(h); });
+}
+
+mgr_status mgr_get_convergence(mgr_handle *h, double *fnc, double *rcm, double *max_rel) {
+    return run(h, [&] {
+        read_stats(h);
+        if (fnc) *fnc = h->h_stats[0];
+        if (rcm) *rcm = h->h_stats[1];
+        if (max_rel) *max_rel = h->h_stats[2];
+    });
+}
+
+mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts,
+                                         int64_t *iterations, double *err_max_hist) {
+    bool not_converged = false;
+    const mgr_status s = run(h, [&] {
+        need(opts != nullptr, MGR_ERR_INVALID_ARG, "NULL options");
+        need(opts->max_iter >= 1, MGR_ERR_INVALID_ARG, "max_iter must be >= 1");
+        need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
+        need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+        int64_t iteration = 0, normal = 0;
+        bool more = true;
+        while (more && iteration < opts->max_iter) {
+            iteration++;
+            if (opts->use_ng && normal == 4) {
+                do_ng(h);
+                normal = 0;
+            } else {
+                do_solve(h, opts->precision);
+                ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
+                do_stateq(h);
+                normal++;
+            }
+            const double fnc = h->h_stats[0], mx = h->h_stats[2];
+            if (err_max_hist) err_max_hist[iteration - 1] = mx;
+            more = opts->tol_max_rel > 0.0 ? !(mx < opts->tol_max_rel) : (fnc > 0.005);
+        }
+        if (iterations) *iterations = iteration;
+        not_converged = more;
+        if (more) h->err = "maximum number of iterations reached";
+    });
+    if (s == MGR_OK && not_converged) return MGR_ERR_NOT_CONVERGED;
+    return s;
+}
+
+mgr_status mgr_set_populations(mgr_handle *h, const double *pop) {
+    return run(h, [&] {
+        need(h->model_loaded && pop, MGR_ERR_INVALID_ARG, "no model or NULL input");
+        ck(cudaMemcpy(h->pop, pop, h->N * h->nlev * sizeof(double), cudaMemcpyHostToDevice), "h2d");
+        ck(launch_emissivity_opacity(h->mv, level_args(h), h->stream), "emissivity");
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        h->pops_valid = true;
+    });
+}
+
+#define MGR_GETTER(NAME, PTR, COUNT)                                                          \
+    mgr_status NAME(mgr_handle *h, double *out) {                                             \
+        return run(h, [&] {                                                                   \
+            need(h->model_loaded && out, MGR_ERR_INVALID_ARG, "no model or NULL output");     \
+            need(PTR != nullptr, MGR_ERR_STATE, "not computed");                              \
+            ck(cudaStreamSynchronize(h->stream), "sync");                                     \
+            ck(cudaMemcpy(out, PTR, (size_t)(COUNT) * sizeof(double), cudaMemcpyDeviceToHost), \
+               "d2h");                                                                        \
+        });                                                                                   \
+    }
+
+MGR_GETTER(mgr_get_populations, h->pop, h->N * h->nlev)
+MGR_GETTER(mgr_get_J, h->J, h->N * (int64_t)h->nfreqs)
+MGR_GETTER(mgr_get_Jlin, h->Jlin, h->N * h->nrad)
+MGR_GETTER(mgr_get_Jeff, h->Jeff, h->N * h->nrad)
+MGR_GETTER(mgr_get_lambda, h->Lam, h->N * h->nrad)
+
+mgr_status mgr_get_emissivity_opacity(mgr_handle *h, double *eta, double *chi) {
+    return run(h, [&] {
+        need(h->model_loaded && eta && chi, MGR_ERR_INVALID_ARG, "no model or NULL output");
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        ck(cudaMemcpy(eta, h->eps, h->N * h->nrad * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(chi, h->kap, h->N * h->nrad * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+    });
+}
+
+mgr_status mgr_get_frequencies(mgr_handle *h, double *nu) {
+    return run(h, [&] {
+        need(h->model_loaded && nu, MGR_ERR_INVALID_ARG, "no model or NULL output");
+        std::vector<double> pw(h->N), line(h->nrad), roots(h->nquads);
+        ck(cudaMemcpy(pw.data(), h->mv.pw, h->N * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(line.data(), h->mv.line, h->nrad * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(roots.data(), h->mv.roots, h->nquads * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        for (int64_t p = 0; p < h->N; p++)
+            for (int k = 0; k < h->nrad; k++) {
+                volatile double w = line[k] * pw[p];
+                for (int z = 0; z < h->nquads; z++) {
+                    volatile double a = w * roots[z];
+                    nu[(p * h->nrad + k) * h->nquads + z] = line[k] + a;
+                }
+            }
+    });
+}
+
+mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates) {
+    return run(h, [&] {
+        if (ms) *ms = h->last_solve_ms;
+        if (updates) *updates = h->last_updates;
+    });
+}
+
+mgr_status mgr_synchronize(mgr_handle *h) {
+    return run(h, [&] { ck(cudaStreamSynchronize(h->stream), "sync"); });
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+// mgr_internal.cuh -- shared definitions of the B200 radiation hot path.
+//
+// Device layout (all arrays resident in HBM for the handle's lifetime):
+//   geometry   pos[3N], vel[3N] (double, AoS), nbr_off[N+1], nbr[.] (int32),
+//              boundary[N] (uint8), cell2bdy[N] (int32, -1 if none),
+//              rays[3R], dshift_max[N], pw[N] (profile width over c)
+//   lines      line[K] (ascending Hz), inv_line[K], A[K], window lo/hi[K]
+//   state      pop/prev1..3 [N*nlev], eps/kap [N*K] (double),
+//              Ehat/Khat [N*K] (float, scaled), Jlin/Lam/Jeff [N*K]
+//   traces     per (direction, origin): offset (int64), length (int32);
+//              points as cell (int32), shift (double), dZ (double)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/magritte_b200.h"
+
+namespace mgr {
+
+// Physical constants with the reference's literals and folding order
+// (src/Tools/constants.hpp:25-46).
+constexpr double kCC = 2.99792458E+8;
+constexpr double kHH = 6.62607004E-34;
+constexpr double kKB = 1.38064852E-23;
+constexpr double kAMU = 1.66053904E-27;
+constexpr double kT_CMB = 2.7254800;
+constexpr double kC_SQUARED = 8.98755179E+16;
+constexpr double kPI = 3.14159265358979323846;
+constexpr double kFOUR_PI = 4.0 * kPI;
+constexpr double kINVERSE_SQRT_PI = 0.5 * 1.12837916709551257390;  // 0.5*M_2_SQRTPI
+constexpr double kTWO_KB_OVER_AMU_C_SQUARED = 2.0 * kKB / (kAMU * kC_SQUARED);
+constexpr double kTWO_HH_OVER_CC_SQUARED = 2.0 * kHH / kC_SQUARED;
+constexpr double kHH_OVER_KB = kHH / kKB;
+constexpr double kHH_OVER_FOUR_PI = kHH / kFOUR_PI;
+
+constexpr int kWarp = 32;
+constexpr int kMaxLevels = 32;     // rate-equation solver: one lane per level
+constexpr int kMaxColpar = 4;
+
+// ------------------------------------------------------------------------
+// Separately rounded double arithmetic (no FMA contraction): the tracer must
+// reproduce the oracle's bits, which rounds every operation on its own.
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rdiv(double a, double b) { return __ddiv_rn(a, b); }
+// (x x' + y y') + z z' -- the dot-product order the oracle restates for
+// Eigen's Vector3d::dot.
+__device__ __forceinline__ double rdot3(double ax, double ay, double az,
+                                        double bx, double by, double bz) {
+    return radd(radd(rmul(ax, bx), rmul(ay, by)), rmul(az, bz));
+}
+
+// Planck function (Functions/planck.tpp:15-23).
+__device__ __forceinline__ double planck(double T, double nu) {
+    const double h_over_kbT = kHH_OVER_KB / T;
+    return kTWO_HH_OVER_CC_SQUARED * (nu * nu * nu) / expm1(h_over_kbT * nu);
+}
+
+// ------------------------------------------------------------------------
+struct ColparDev {
+    int ntmp, ncol, ortho_para;
+    int32_t *icol, *jcol;   // [ncol]
+    double *tmp;            // [ntmp]
+    double *Cd, *Ce;        // [ntmp*ncol]
+    double *abn;            // [N]
+};
+
+// Non-owning view of the device model handed to kernels by value.
+struct ModelView {
+    int64_t N;
+    int nrays, npairs, nlev, nrad, nquads, nfreqs, ncolpar;
+    const double *pos, *vel, *rays, *ray_w;
+    const int32_t *nbr_off, *nbr;
+    const uint8_t *boundary;
+    const int32_t *cell2bdy;
+    const int32_t *antipod;
+    const double *bdy_T;
+    const double *T, *dshift_max, *pw, *inv_pw;
+    const double *line, *inv_line, *A, *Bs, *Ba, *energy, *weight;
+    const int32_t *irad, *jrad, *win_lo, *win_hi;
+    const double *roots, *qw;
+    const double *pop_tot;
+    ColparDev colpar[kMaxColpar];
+    double pop_prec;
+};
+
+// Trace store for one batch of origins [o_begin, o_begin + o_count).
+struct TraceView {
+    int64_t o_begin, o_count;
+    int ndir;
+    const int64_t *off;    // [ndir*o_count]
+    const int32_t *len;    // [ndir*o_count]
+    const int32_t *cell;
+    const double *shift, *dZ;
+};
+
+// Error counters written by kernels (bounded, never trap).
+struct DevFlags {
+    unsigned long long trace_err;   // rays without a neighbour ahead
+    unsigned long long interp_err;  // > 10000 interpolation points
+    unsigned long long lu_err;      // zero pivots
+    unsigned long long cap_err;     // trace longer than its slot
+    unsigned long long stuck_err;   // step limit reached
+};
+
+// ------------------------------------------------------------------------
+// Host-side launchers (each file owns its kernels).
+cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_count,
+                               int32_t *len, DevFlags *flags, cudaStream_t s);
+cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
+                              double *shift, double *dZ, DevFlags *flags, cudaStream_t s);
+
+struct SolveArgs {
+    const double *eps, *kap;        // [N*K] emissivity, opacity (FP64 path)
+    const float2 *ehat_khat;        // [N*K] scaled (mixed path)
+    double mixed_scale;             // power of two applied to Ehat/Khat
+    double *Jlin, *Lam;             // [N*K]
+    double *J;                      // [N*nfreqs] or null
+    int warps_per_block;
+};
+cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const SolveArgs &a,
+                                int precision, DevFlags *flags, cudaStream_t s);
+
+struct LevelArgs {
+    double *pop, *prev1, *prev2, *prev3;   // [N*nlev]
+    double *eps, *kap;                     // [N*K]
+    float2 *ehat_khat;                     // [N*K]
+    double mixed_scale;
+    double *Jlin, *Lam, *Jeff;             // [N*K]
+    double *partials;                      // reduction scratch
+    double *stats;                         // [8] device results
+    int npartials;
+};
+cudaError_t launch_lte(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+cudaError_t launch_emissivity_opacity(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+cudaError_t launch_jeff(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+cudaError_t launch_stateq(const ModelView &m, const LevelArgs &a, DevFlags *flags, cudaStream_t s);
+cudaError_t launch_convergence(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+cudaError_t launch_ng(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+int level_partials_needed(const ModelView &m);
+
+}  // namespace mgr

@@ -1,0 +1,207 @@
+// trace.cu -- ray tracing through the neighbour graph on the device.
+//
+// One thread walks one (direction, origin) ray, as Geometry::trace_ray
+// <CoMoving> does (Model/Geometry/geometry.tpp:21-95): at each step it picks,
+// among the current cell's neighbours that lie further along the ray, the
+// one closest to the ray (get_next_general, :328-421), then records the
+// projected point, inserting Doppler interpolation points where the shift
+// jump exceeds dshift_max (set_data, :100-207).  Every double operation is
+// separately rounded (__dmul_rn/__dadd_rn/...) so the traced cell sequence,
+// shifts and increments are bit-identical to the oracle's.
+//
+// Two passes over the same walk: a counting pass sizes each trace, a prefix
+// sum places it, a filling pass writes it.  Threads of a warp take 32
+// consecutive origins of one direction, which on a lattice walk in step.
+// The walk is bounded by the cell count (Z grows strictly, so no cell can
+// repeat); failures are counted in DevFlags, never trapped.
+#include "mgr_internal.cuh"
+
+namespace mgr {
+
+namespace {
+
+struct Walker {
+    const ModelView &m;
+    int64_t origin;
+    double rx, ry, rz;
+    double ox, oy, oz;       // origin position
+    double vox, voy, voz;    // origin velocity
+
+    __device__ Walker(const ModelView &mv, int64_t o, int d) : m(mv), origin(o) {
+        rx = m.rays[3 * d + 0]; ry = m.rays[3 * d + 1]; rz = m.rays[3 * d + 2];
+        ox = m.pos[3 * o + 0]; oy = m.pos[3 * o + 1]; oz = m.pos[3 * o + 2];
+        vox = m.vel[3 * o + 0]; voy = m.vel[3 * o + 1]; voz = m.vel[3 * o + 2];
+    }
+
+    // Geometry::get_doppler_shift<CoMoving> (geometry.tpp:443-446)
+    __device__ __forceinline__ double shift(int64_t c) const {
+        const double dx = rsub(m.vel[3 * c + 0], vox);
+        const double dy = rsub(m.vel[3 * c + 1], voy);
+        const double dz = rsub(m.vel[3 * c + 2], voz);
+        return rsub(1.0, rdot3(dx, dy, dz, rx, ry, rz));
+    }
+
+    // Geometry::get_next_general (geometry.tpp:328-421)
+    __device__ __forceinline__ int64_t next(int64_t current, double &Z, double &dZ) const {
+        double dmin = 1.7976931348623157e308;   // numeric_limits<double>::max()
+        int64_t nxt = -1;
+        const int32_t b = m.nbr_off[current], e = m.nbr_off[current + 1];
+        for (int32_t k = b; k < e; k++) {
+            const int32_t nb = __ldg(m.nbr + k);
+            const double Rx = rsub(__ldg(m.pos + 3 * nb + 0), ox);
+            const double Ry = rsub(__ldg(m.pos + 3 * nb + 1), oy);
+            const double Rz = rsub(__ldg(m.pos + 3 * nb + 2), oz);
+            const double Z_new = rdot3(Rx, Ry, Rz, rx, ry, rz);
+            if (Z_new > Z) {
+                const double d2 = rsub(rdot3(Rx, Ry, Rz, Rx, Ry, Rz), rmul(Z_new, Z_new));
+                if (d2 < dmin) {
+                    dmin = d2;
+                    nxt = nb;
+                    dZ = rsub(Z_new, Z);
+                }
+            }
+        }
+        Z = radd(Z, dZ);
+        return nxt;
+    }
+};
+
+// Sink that only counts points.
+struct CountSink {
+    int64_t n = 0;
+    __device__ __forceinline__ void push(int64_t, double, double) { n++; }
+};
+
+// Sink that writes points into the slot [base, base+cap).
+struct WriteSink {
+    int64_t n = 0, cap, base;
+    int32_t *cell;
+    double *shift, *dZ;
+    bool over = false;
+    __device__ __forceinline__ void push(int64_t c, double s, double z) {
+        if (n < cap) {
+            cell[base + n] = (int32_t)c;
+            shift[base + n] = s;
+            dZ[base + n] = z;
+        } else {
+            over = true;
+        }
+        n++;
+    }
+};
+
+// Geometry::set_data (geometry.tpp:100-207); returns false on > 10000
+// interpolation points.
+template <class Sink>
+__device__ __forceinline__ bool set_data(int64_t crt, int64_t nxt, double shift_crt,
+                                         double shift_nxt, double dZ_loc, double dshift_max,
+                                         Sink &sink) {
+    const double dshift = rsub(shift_nxt, shift_crt);
+    const double dshift_abs = fabs(dshift);
+    if (dshift_abs > dshift_max) {
+        const double q = radd(rdiv(dshift_abs, dshift_max), 1.0);
+        if (!(q <= 10000.5)) return false;          // also catches NaN
+        const long long n_interpl = (long long)q;
+        const long long half_n_interpl = (long long)rmul(0.5, (double)n_interpl);
+        const double dZ_interpl = rdiv(dZ_loc, (double)n_interpl);
+        const double dshift_interpl = rdiv(dshift, (double)n_interpl);
+        if (n_interpl > 10000 || n_interpl < 0) return false;
+        for (long long k = 1; k < half_n_interpl; k++)
+            sink.push(crt, radd(shift_crt, rmul((double)k, dshift_interpl)), dZ_interpl);
+        for (long long k = half_n_interpl; k <= n_interpl; k++)
+            sink.push(nxt, radd(shift_crt, rmul((double)k, dshift_interpl)), dZ_interpl);
+    } else {
+        sink.push(nxt, shift_nxt, dZ_loc);
+    }
+    return true;
+}
+
+// Geometry::trace_ray<CoMoving> (geometry.tpp:21-95).  Returns 0 or an
+// error code: 1 no neighbour ahead, 2 too many interpolation points,
+// 3 step limit.
+template <class Sink>
+__device__ int walk(const ModelView &m, int64_t o, int d, Sink &sink) {
+    const Walker w(m, o, d);
+    const double dsm = m.dshift_max[o];
+    double Z = 0.0, dZ = 0.0;
+    int64_t nxt = w.next(o, Z, dZ);
+    if (nxt == -1) return 0;
+    int64_t crt = o;
+    double shift_crt = w.shift(crt);
+    double shift_nxt = w.shift(nxt);
+    if (!set_data(crt, nxt, shift_crt, shift_nxt, dZ, dsm, sink)) return 2;
+    int64_t steps = 0;
+    while (!m.boundary[nxt]) {
+        if (++steps > m.N) return 3;
+        shift_crt = shift_nxt;
+        crt = nxt;
+        nxt = w.next(nxt, Z, dZ);
+        if (nxt < 0) return 1;
+        shift_nxt = w.shift(nxt);
+        if (!set_data(crt, nxt, shift_crt, shift_nxt, dZ, dsm, sink)) return 2;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ void count_error(DevFlags *f, int code) {
+    if (code == 1) atomicAdd(&f->trace_err, 1ull);
+    else if (code == 2) atomicAdd(&f->interp_err, 1ull);
+    else if (code == 3) atomicAdd(&f->stuck_err, 1ull);
+}
+
+__global__ void __launch_bounds__(128) trace_count_kernel(ModelView m, int64_t o_begin,
+                                                          int64_t o_count, int32_t *len,
+                                                          DevFlags *flags) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = (int64_t)m.nrays * o_count;
+    if (idx >= total) return;
+    const int d = (int)(idx / o_count);
+    const int64_t o = o_begin + idx % o_count;
+    CountSink sink;
+    const int code = walk(m, o, d, sink);
+    if (code) count_error(flags, code);
+    len[idx] = code ? 0 : (int32_t)sink.n;
+}
+
+__global__ void __launch_bounds__(128) trace_fill_kernel(ModelView m, TraceView t,
+                                                         int32_t *cell, double *shift,
+                                                         double *dZ, DevFlags *flags) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t total = (int64_t)t.ndir * t.o_count;
+    if (idx >= total) return;
+    const int d = (int)(idx / t.o_count);
+    const int64_t o = t.o_begin + idx % t.o_count;
+    WriteSink sink;
+    sink.cap = t.len[idx];
+    sink.base = t.off[idx];
+    sink.cell = cell;
+    sink.shift = shift;
+    sink.dZ = dZ;
+    const int code = walk(m, o, d, sink);
+    if (code) count_error(flags, code);
+    if (sink.over || (code == 0 && sink.n != sink.cap)) atomicAdd(&flags->cap_err, 1ull);
+}
+
+}  // namespace
+
+cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_count,
+                               int32_t *len, DevFlags *flags, cudaStream_t s) {
+    const int64_t total = (int64_t)m.nrays * o_count;
+    if (total == 0) return cudaSuccess;
+    const int threads = 128;
+    const int64_t blocks = (total + threads - 1) / threads;
+    trace_count_kernel<<<(unsigned)blocks, threads, 0, s>>>(m, o_begin, o_count, len, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
+                              double *shift, double *dZ, DevFlags *flags, cudaStream_t s) {
+    const int64_t total = (int64_t)t.ndir * t.o_count;
+    if (total == 0) return cudaSuccess;
+    const int threads = 128;
+    const int64_t blocks = (total + threads - 1) / threads;
+    trace_fill_kernel<<<(unsigned)blocks, threads, 0, s>>>(m, t, cell, shift, dZ, flags);
+    return cudaGetLastError();
+}
+
+}  // namespace mgr

@@ -1,0 +1,212 @@
+"""``Simulation``: the reference's Python-facing interface over the C ABI.
+
+Method names and their meaning follow ``magritte.core.Simulation``
+(``src/bindings/pyBindings.cpp:404-449``): a user calls
+
+    sim = Simulation(model)
+    sim.compute_spectral_discretisation()
+    sim.compute_boundary_intensities()
+    sim.compute_LTE_level_populations()
+    sim.compute_radiation_field()            # or compute_level_populations()
+
+as in ``tests/integration/test_0_1D_all_constant.py:64-99``.  Every call goes
+to hand-written sm_100a kernels through ``libmagritte_b200.so``; errors come
+back as :class:`MagritteError` with the C status code.  Differences from the
+reference: the model is passed as a :class:`magritte_b200.model.Model`
+instead of an ``Io`` object, and ``compute_level_populations`` takes the
+options that the ``Io`` overloads fix (Ng, iteration cap) plus the
+precision and an optional max-relative-change tolerance.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _capi
+from ._capi import MagritteError, MGR_FP64, MGR_MIXED
+
+_PREC = {"fp64": MGR_FP64, "mixed": MGR_MIXED, MGR_FP64: MGR_FP64, MGR_MIXED: MGR_MIXED}
+
+
+class Simulation:
+    def __init__(self, model=None, device: int = 0):
+        self._lib = _capi.load()
+        h = C.c_void_p()
+        st = self._lib.mgr_create(device, C.byref(h))
+        if st != 0:
+            raise MagritteError(st, "mgr_create failed (no CUDA device?)")
+        self._h = h
+        self.model = None
+        self.error_max = []
+        self.error_mean = []
+        self.fraction_not_converged = []
+        if model is not None:
+            self.read(model)
+
+    # ------------------------------------------------------------ plumbing
+    def _ck(self, st: int):
+        if st != 0 and st != 4:
+            raise MagritteError(st, self._lib.mgr_last_error(self._h).decode())
+        return st
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.mgr_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --------------------------------------------------------------- model
+    def read(self, model):
+        """Uploads the model (replaces ``Model::read(io)``)."""
+        desc, keep = _capi.make_desc(model)
+        self._ck(self._lib.mgr_upload_model(self._h, C.byref(desc)))
+        self.model = model
+        return 0
+
+    def set_trace_budget(self, nbytes: int):
+        self._ck(self._lib.mgr_set_trace_budget(self._h, int(nbytes)))
+
+    # ---------------------------------------------------- reference calls
+    def compute_spectral_discretisation(self) -> int:
+        return self._ck(self._lib.mgr_compute_spectral_discretisation(self._h))
+
+    def compute_boundary_intensities(self) -> int:
+        return self._ck(self._lib.mgr_compute_boundary_intensities(self._h))
+
+    def compute_LTE_level_populations(self) -> int:
+        return self._ck(self._lib.mgr_compute_LTE_level_populations(self._h))
+
+    def compute_radiation_field(self, precision="fp64", keep_J: Optional[bool] = None) -> int:
+        if keep_J is not None:
+            self._ck(self._lib.mgr_set_keep_J(self._h, int(bool(keep_J))))
+        return self._ck(self._lib.mgr_compute_radiation_field(self._h, _PREC[precision]))
+
+    def compute_Jeff(self):
+        self._ck(self._lib.mgr_compute_Jeff(self._h))
+
+    def compute_level_populations_from_stateq(self):
+        self._ck(self._lib.mgr_compute_level_populations_from_stateq(self._h))
+        self._record()
+
+    def ng_acceleration(self):
+        self._ck(self._lib.mgr_ng_acceleration(self._h))
+        self._record()
+
+    def compute_level_populations(self, use_Ng: bool = True, max_niterations: int = 1000,
+                                  precision="fp64", tol_max_rel: float = 0.0) -> int:
+        """ALI loop (``Simulation::compute_level_populations``,
+        ``sim_lines.tpp:61-164``); returns the iteration count.
+        ``tol_max_rel`` > 0 stops at max relative population change < tol."""
+        o = _capi.AliOpts()
+        o.use_ng = int(bool(use_Ng))
+        o.precision = _PREC[precision]
+        o.max_iter = int(max_niterations)
+        o.tol_max_rel = float(tol_max_rel)
+        o.use_graph = 0
+        it = C.c_int64(0)
+        hist = np.zeros(max(1, int(max_niterations)))
+        st = self._ck(self._lib.mgr_compute_level_populations(self._h, C.byref(o), C.byref(it),
+                                                              _capi.ptr(hist)))
+        self.error_max = list(hist[: it.value])
+        self.converged = (st == 0)
+        return int(it.value)
+
+    def get_npoints_on_rays_comoving(self) -> np.ndarray:
+        m = self.model
+        out = np.zeros((m.nrays // 2, m.ncells), dtype=np.int64)
+        self._ck(self._lib.mgr_get_npoints_on_rays(self._h, _capi.ptr(out)))
+        return out
+
+    get_npoints_on_rays = get_npoints_on_rays_comoving
+
+    # --------------------------------------------------------- accessors
+    def trace(self):
+        self._ck(self._lib.mgr_trace(self._h))
+
+    def trace_ray(self, o: int, r: int):
+        n = C.c_int64(0)
+        self._ck(self._lib.mgr_get_trace(self._h, o, r, 0, None, None, None, C.byref(n)))
+        cap = max(1, n.value)
+        cell = np.zeros(cap, dtype=np.int64)
+        shift = np.zeros(cap)
+        dZ = np.zeros(cap)
+        self._ck(self._lib.mgr_get_trace(self._h, o, r, cap, _capi.ptr(cell), _capi.ptr(shift),
+                                         _capi.ptr(dZ), C.byref(n)))
+        return cell[: n.value], shift[: n.value], dZ[: n.value]
+
+    def _get(self, fn, shape):
+        out = np.zeros(shape)
+        self._ck(fn(self._h, _capi.ptr(out)))
+        return out
+
+    @property
+    def population(self) -> np.ndarray:
+        m = self.model
+        return self._get(self._lib.mgr_get_populations, (m.ncells, m.linedata.nlev))
+
+    @population.setter
+    def population(self, pop: np.ndarray):
+        pop = np.ascontiguousarray(pop, dtype=np.float64)
+        self._ck(self._lib.mgr_set_populations(self._h, _capi.ptr(pop)))
+
+    @property
+    def J(self) -> np.ndarray:
+        m = self.model
+        return self._get(self._lib.mgr_get_J, (m.ncells, m.nfreqs))
+
+    @property
+    def Jlin(self) -> np.ndarray:
+        m = self.model
+        return self._get(self._lib.mgr_get_Jlin, (m.ncells, m.nlines))
+
+    @property
+    def Jeff(self) -> np.ndarray:
+        m = self.model
+        return self._get(self._lib.mgr_get_Jeff, (m.ncells, m.nlines))
+
+    @property
+    def Lambda(self) -> np.ndarray:
+        """Diagonal ALO element Ls[p][k] (nr == p)."""
+        m = self.model
+        return self._get(self._lib.mgr_get_lambda, (m.ncells, m.nlines))
+
+    @property
+    def frequencies(self) -> np.ndarray:
+        m = self.model
+        return self._get(self._lib.mgr_get_frequencies, (m.ncells, m.nfreqs))
+
+    def emissivity_opacity(self):
+        m = self.model
+        e = np.zeros((m.ncells, m.nlines))
+        c = np.zeros((m.ncells, m.nlines))
+        self._ck(self._lib.mgr_get_emissivity_opacity(self._h, _capi.ptr(e), _capi.ptr(c)))
+        return e, c
+
+    def convergence(self):
+        f, r, x = C.c_double(), C.c_double(), C.c_double()
+        self._ck(self._lib.mgr_get_convergence(self._h, C.byref(f), C.byref(r), C.byref(x)))
+        return f.value, r.value, x.value
+
+    def _record(self):
+        f, r, x = self.convergence()
+        self.fraction_not_converged.append(f)
+        self.error_mean.append(r)
+        self.error_max.append(x)
+
+    def solve_stats(self):
+        ms, up = C.c_double(), C.c_double()
+        self._ck(self._lib.mgr_get_solve_stats(self._h, C.byref(ms), C.byref(up)))
+        return ms.value, up.value

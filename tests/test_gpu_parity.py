@@ -1,0 +1,150 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances: traced points are bit-exact; J, Jlin, the ALO and level
+populations agree to 1e-6 relative in FP64 mode (the measured gap is
+~1e-12: the device elimination is algebraically the reference's but rounds
+differently) and to 1e-4 in mixed mode.
+"""
+import numpy as np
+import pytest
+
+import magritte_b200.model as M
+from magritte_b200 import Simulation
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+FP64_RTOL = 1e-6
+MIXED_RTOL = 1e-4
+
+
+def rel_err(a, b, floor=0.0):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    den = np.maximum(np.abs(b), floor)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r = np.abs(a - b) / den
+    r[(a == b)] = 0.0
+    return float(np.nanmax(r)) if r.size else 0.0
+
+
+def small_wind(n=10, nlev=5, seed=7):
+    return M.wind_model(n, seed=seed, nlev=nlev, nside=1, name=f"wind{n}")
+
+
+def broken_lattice():
+    """6^3 lattice whose interior cell (2,2,2) has an empty neighbour list:
+    every ray that enters it finds no neighbour ahead."""
+    model = M.lattice_cloud(6, name="broken")
+    p = 2 + 6 * (2 + 6 * 2)
+    offs = model.nbr_offsets.copy()
+    a, b = int(offs[p]), int(offs[p + 1])
+    model.nbr_list = np.concatenate([model.nbr_list[:a], model.nbr_list[b:]])
+    offs[p + 1:] -= (b - a)
+    model.nbr_offsets = offs
+    return model
+
+
+def setup_pair(model, keep_J=True):
+    sim = Simulation(model)
+    sim.compute_spectral_discretisation()
+    sim.compute_boundary_intensities()
+    sim.compute_LTE_level_populations()
+    orc = oracle.Oracle(model).setup()
+    if keep_J:
+        sim.compute_radiation_field("fp64", keep_J=True)
+    return sim, orc
+
+
+@pytest.mark.parametrize("make", [M.config1, lambda: small_wind(10, 5, 7),
+                                  lambda: M.wind_model(9, seed=3, nlev=4, nside=2, vmax=40e3)])
+def test_traces_bit_exact(gpu, make):
+    model = make()
+    sim = Simulation(model)
+    orc = oracle.Oracle(model)
+    sim.trace()
+    rng = np.random.default_rng(0)
+    origins = rng.choice(model.ncells, size=min(model.ncells, 120), replace=False)
+    for o in origins:
+        for r in range(model.nrays):
+            c1, s1, z1 = sim.trace_ray(int(o), r)
+            c2, s2, z2 = orc.trace_ray(int(o), r)
+            assert np.array_equal(c1, c2), (o, r)
+            assert np.array_equal(s1, s2), (o, r)
+            assert np.array_equal(z1, z2), (o, r)
+
+
+def test_npoints_on_rays(gpu):
+    model = small_wind(8, 4, 11)
+    sim = Simulation(model)
+    orc = oracle.Oracle(model)
+    assert np.array_equal(sim.get_npoints_on_rays(), orc.get_npoints_on_rays())
+
+
+@pytest.mark.parametrize("make", [M.config1, lambda: small_wind(10, 5, 7), M.config3])
+def test_radiation_field_fp64(gpu, make):
+    model = make()
+    sim, orc = setup_pair(model)
+    orc.compute_radiation_field()
+    assert orc.trace_errors == 0
+    J = sim.J
+    assert rel_err(J, orc.J) < FP64_RTOL
+    orc.compute_Jeff()
+    assert rel_err(sim.Jlin, orc.Jlin) < FP64_RTOL
+    assert rel_err(sim.Lambda, orc.Ls) < FP64_RTOL
+    sim.compute_Jeff()
+    assert rel_err(sim.Jeff, orc.Jeff, floor=1e-3 * np.abs(orc.Jlin).max()) < FP64_RTOL
+
+
+def test_radiation_field_subset_config2_shape(gpu):
+    """The 64^3 wind at full size: J line integrals and ALO at a sample of
+    origins against the oracle (which solves only those origins)."""
+    model = M.config2()
+    sim = Simulation(model)
+    sim.compute_spectral_discretisation()
+    sim.compute_boundary_intensities()
+    sim.compute_LTE_level_populations()
+    sim.compute_radiation_field("fp64")
+    orc = oracle.Oracle(model).setup()
+    rng = np.random.default_rng(1)
+    origins = np.sort(rng.choice(model.ncells, size=24, replace=False))
+    orc.compute_radiation_field(origins=origins)
+    orc.compute_Jeff()
+    assert rel_err(sim.Jlin[origins], orc.Jlin[origins]) < FP64_RTOL
+    assert rel_err(sim.Lambda[origins], orc.Ls[origins]) < FP64_RTOL
+
+
+def test_stateq_and_ng_iterations(gpu):
+    """Eight ALI iterations (one of them Ng) against the oracle."""
+    model = small_wind(10, 5, 7)
+    sim, orc = setup_pair(model, keep_J=False)
+    it_gpu = sim.compute_level_populations(use_Ng=True, max_niterations=8, precision="fp64",
+                                           tol_max_rel=1e-30)
+    it_cpu, hist = orc.compute_level_populations(use_ng=True, max_iter=8, tol_max_rel=1e-30)
+    assert it_gpu == it_cpu == 8
+    pop_g = sim.population
+    assert rel_err(pop_g, orc.pop, floor=1e-10 * model.population_tot.max()) < FP64_RTOL
+    assert np.allclose(sim.error_max, hist, rtol=1e-4, atol=1e-12)
+
+
+def test_ali_converges_config1_density(gpu):
+    """Full ALI + Ng to 1e-4 on the lattice cloud; same iteration count and
+    populations as the oracle."""
+    model = M.lattice_cloud(10, name="lattice10")
+    sim, orc = setup_pair(model, keep_J=False)
+    it_gpu = sim.compute_level_populations(True, 200, "fp64", tol_max_rel=1e-4)
+    it_cpu, _ = orc.compute_level_populations(True, 200, 1e-4)
+    assert sim.converged
+    assert abs(it_gpu - it_cpu) <= 1
+    assert rel_err(sim.population, orc.pop) < 1e-4
+
+
+def test_errors_are_status_codes(gpu):
+    """A neighbour list with a dead end yields MGR_ERR_TRACE, not a fault."""
+    from magritte_b200 import MagritteError
+    model = broken_lattice()
+    sim = Simulation(model)
+    with pytest.raises(MagritteError) as e:
+        sim.trace()
+    assert e.value.status == 2
