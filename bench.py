@@ -1,0 +1,336 @@
+"""Benchmark: ALI iterations and wall-clock to 1e-4 populations on one B200.
+
+Workload (default): the 64^3 jittered spherical wind (262,144 cells, 10-level
+linear rotor, 9 lines x 31 bins = 279 bins, 48 HEALPix rays = 24 pairs),
+seeded synthetic data.  One step is one complete solve of the hot path:
+trace every ray, start from LTE populations, and iterate formal solve +
+Jeff + statistical equilibrium (+ Ng every 5th iteration) until the max
+relative population change over all (cell, level) with n > 1e-10 n_tot
+drops below 1e-4.
+
+    value  seconds per converged solve, device-timed (CUDA events on the
+           library's stream), model already resident in HBM
+    e2e    the same through the C ABI from host buffers: model upload,
+           set-up, trace, ALI, download of the populations, all timed
+    roofline  the formal-solve kernel: algorithmic bytes (44 B per
+           ray-point-frequency update in FP64, 24 B in mixed) / its average
+           launch time, against the measured HBM copy bandwidth
+    cpu_baseline  the CPU oracle on this host's cores: one formal solve on a
+           sample of origins, extrapolated, plus the full rate-equation step,
+           times the iteration count of the solve
+
+``--impl reference`` times the CPU oracle (the reference's algorithm
+restated in C, OpenMP over origins as the reference does) the same way and
+prints one line with "impl": "reference".
+
+Multi-GPU (torchrun): every rank solves its own replica (no exchange on
+the data path); value is the job's max time over ranks divided by the
+number of solves.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ALI iters & wall-clock to 1e-4 pops on 1 B200: learned+FP32 vs plain FP64"
+TOL = 1.0e-4
+MAX_ITER = 400
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="wind64", choices=["wind64", "lattice16"])
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_model(name):
+    import magritte_b200.model as M
+    if name == "wind64":
+        return M.config2()
+    return M.config1()
+
+
+def workload_config(name, model, prec):
+    return {"workload": "64^3 spherical wind, 10-level rotor" if name == "wind64"
+            else "16^3 lattice cloud, 2-level line",
+            "cells": model.ncells, "levels": model.linedata.nlev, "lines": model.nlines,
+            "bins_per_line": model.nquads, "rays": model.nrays,
+            "start": "LTE", "tol_max_rel": TOL, "ng": True, "precision": prec,
+            "l2": "inputs larger than L2 (ray traces of several GB re-read every iteration)"}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------------ CPU arm
+
+def cpu_oracle_time(model, iterations, sample_s, nthreads=None):
+    """The CPU oracle on this host: a formal solve over a seeded sample of
+    origins (all ray pairs), scaled to all origins, plus one full
+    rate-equation step, times the iteration count."""
+    import numpy as np
+    import oracle
+    nthreads = nthreads or os.cpu_count() or 1
+    o = oracle.Oracle(model).setup()
+    rng = np.random.default_rng(0)
+    n = 64
+    t_solve = None
+    while True:
+        origins = np.sort(rng.choice(model.ncells, size=min(n, model.ncells), replace=False))
+        t0 = time.perf_counter()
+        o.compute_radiation_field(origins=origins, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        if dt > 0.25 * sample_s or n >= model.ncells:
+            t_solve = dt * model.ncells / len(origins)
+            break
+        n = min(model.ncells, int(n * max(2.0, 0.3 * sample_s / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    o.compute_Jeff()
+    o.compute_level_populations_from_stateq()
+    t_stateq = time.perf_counter() - t0
+    per_iter = t_solve + t_stateq
+    return {"seconds": per_iter * iterations, "per_iteration_s": per_iter,
+            "formal_solve_s": t_solve, "stateq_s": t_stateq, "sample_origins": int(len(origins)),
+            "cores": nthreads}
+
+
+# iterations of the FP64 solve of the default workload; the reference arm,
+# which cannot afford the full solve on CPU, multiplies its per-iteration
+# time by the count the same algorithm needs (equal iteration counts of
+# the oracle and the device path are checked by the GPU tests).
+REFERENCE_ITERATIONS = {"wind64": None, "lattice16": None}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    model = make_model(args.workload)
+    iters = REFERENCE_ITERATIONS.get(args.workload)
+    if iters is None:
+        import oracle
+        o = oracle.Oracle(model).setup() if args.workload == "lattice16" else None
+        if o is not None:
+            iters, _ = o.compute_level_populations(True, MAX_ITER, TOL)
+        else:
+            iters = int(os.environ.get("MGR_REFERENCE_ITERATIONS", "0")) or 30
+    steps = []
+    info = None
+    for _ in range(args.warmup):
+        pass
+    for _ in range(max(1, args.steps)):
+        info = cpu_oracle_time(model, iters, args.cpu_sample_s)
+        steps.append(info["seconds"])
+    value = statistics.mean(steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": workload_config(args.workload, model, "fp64"),
+        "ali_iterations": iters,
+        "cpu_baseline": {"value": value, "unit": "s", "cores": info["cores"], "kind": "port",
+                         "sample": f"one formal solve over {info['sample_origins']} seeded origins "
+                                   f"x all ray pairs scaled to {model.ncells} origins, plus one "
+                                   f"full rate-equation step, x {iters} iterations"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def run_b200(args):
+    import numpy as np
+    from magritte_b200 import Simulation
+    rank, world, local = dist_env()
+    dist = world > 1
+    if dist:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    model = make_model(args.workload)
+    prec = args.precision
+
+    def one_solve(sim):
+        sim.trace()
+        sim.compute_LTE_level_populations()
+        return sim.compute_level_populations(True, MAX_ITER, prec, tol_max_rel=TOL)
+
+    # ---- device-resident solve
+    sim = Simulation(model, device=local if dist else 0)
+    sim.compute_spectral_discretisation()
+    sim.compute_boundary_intensities()
+    for _ in range(args.warmup):
+        one_solve(sim)
+    if dist:
+        tdist.barrier()
+    launches0 = sim.launch_count()
+    times, iters, solve_ms, solve_upd = [], [], [], []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            sim.timer_start()
+            it = one_solve(sim)
+            times.append(sim.timer_stop() / 1e3)
+            iters.append(it)
+            ms, up = sim.solve_stats()
+            solve_ms.append(ms)
+            solve_upd.append(up)
+    launches = (sim.launch_count() - launches0) // max(1, args.steps)
+    converged = bool(getattr(sim, "converged", False))
+    err_hist = list(sim.error_max)
+    t_step = statistics.mean(times)
+
+    # ---- end to end through the C ABI from host buffers
+    e2e = []
+    h2d = model.nbytes() + sum(int(a.nbytes) for a in (model.linedata.energy,))
+    d2h = model.ncells * model.linedata.nlev * 8
+    for _ in range(max(1, args.steps)):
+        t0 = time.perf_counter()
+        s2 = Simulation(model, device=local if dist else 0)
+        s2.compute_spectral_discretisation()
+        s2.compute_boundary_intensities()
+        s2.compute_LTE_level_populations()
+        s2.compute_level_populations(True, MAX_ITER, prec, tol_max_rel=TOL)
+        pop = s2.population
+        e2e.append(time.perf_counter() - t0)
+        s2.close()
+    assert np.all(np.isfinite(pop))
+
+    # ---- multi-GPU: max over ranks
+    if dist:
+        t = torch.tensor([t_step, statistics.mean(e2e)], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        t_step, e2e_t = float(t[0]), float(t[1])
+        tdist.barrier()
+        tdist.destroy_process_group()
+    else:
+        e2e_t = statistics.mean(e2e)
+    if rank != 0:
+        return
+
+    hbm, kind = peaks()
+    bpu = 44.0 if prec == "fp64" else 24.0
+    avg_ms = statistics.mean(solve_ms)
+    achieved = solve_upd[-1] * bpu / (avg_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": t_step / world, "unit": "s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == "fp64" else "f32+f64",
+        "data": "synthetic (seeded)",
+        "config": workload_config(args.workload, model, prec),
+        "ali_iterations": iters[-1], "converged": converged,
+        "final_max_rel_change": err_hist[-1] if err_hist else None,
+        "formal_solve": {"ms": avg_ms, "updates": solve_upd[-1],
+                         "updates_per_s": solve_upd[-1] / (avg_ms / 1e3)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "note": f"formal-solve kernel; {bpu:.0f} B/update algorithmic; peak "
+                             f"{kind} copy bandwidth"},
+        "e2e": {"value": e2e_t / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline and world == 1:
+        info = cpu_oracle_time(model, iters[-1], args.cpu_sample_s)
+        line["cpu_baseline"] = {
+            "value": info["seconds"], "unit": "s", "cores": info["cores"], "kind": "port",
+            "sample": f"one formal solve over {info['sample_origins']} seeded origins x all ray "
+                      f"pairs scaled to {model.ncells} origins, plus one full rate-equation "
+                      f"step, x {iters[-1]} iterations"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

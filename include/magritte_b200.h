@@ -226,6 +226,17 @@ mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates);
 /* Synchronises the handle's stream. */
 mgr_status mgr_synchronize(mgr_handle *h);
 
+/* Device timing of a region of calls on the handle's stream: start records
+ * a CUDA event, stop records another, waits for it and returns the elapsed
+ * milliseconds.  Benchmark support; no reference counterpart (the reference
+ * times with its host Timer, Tools/timer.hpp:26-143). */
+mgr_status mgr_timer_start(mgr_handle *h);
+mgr_status mgr_timer_stop(mgr_handle *h, double *ms);
+
+/* Number of this library's kernels launched on the handle since it was
+ * created (library kernels such as CUB's prefix sum are not counted). */
+mgr_status mgr_get_launch_count(mgr_handle *h, int64_t *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,7 @@ EXPORTS = (
     "mgr_get_convergence", "mgr_compute_level_populations", "mgr_set_populations",
     "mgr_get_populations", "mgr_get_J", "mgr_get_Jlin", "mgr_get_Jeff", "mgr_get_lambda",
     "mgr_get_emissivity_opacity", "mgr_get_frequencies", "mgr_get_solve_stats",
-    "mgr_synchronize",
+    "mgr_synchronize", "mgr_timer_start", "mgr_timer_stop", "mgr_get_launch_count",
 )
 
 _P = C.c_void_p
@@ -99,8 +99,10 @@ def load(build_if_missing: bool = True):
     for n in ("mgr_compute_spectral_discretisation", "mgr_compute_boundary_intensities",
               "mgr_compute_LTE_level_populations", "mgr_trace", "mgr_compute_Jeff",
               "mgr_compute_level_populations_from_stateq", "mgr_ng_acceleration",
-              "mgr_synchronize"):
+              "mgr_synchronize", "mgr_timer_start"):
         getattr(L, n).argtypes = [_P]
+    L.mgr_timer_stop.argtypes = [_P, C.POINTER(_dbl)]
+    L.mgr_get_launch_count.argtypes = [_P, C.POINTER(_i64)]
     L.mgr_get_npoints_on_rays.argtypes = [_P, _P]
     L.mgr_get_trace.argtypes = [_P, _i64, _i64, _i64, _P, _P, _P, C.POINTER(_i64)]
     L.mgr_compute_radiation_field.argtypes = [_P, _i32]

@@ -44,8 +44,9 @@ __global__ void widen_kernel(const int32_t *in, int64_t *out, int64_t n) {
 struct mgr_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
     std::string err;
+    int64_t launches = 0;
 
     // sizes
     int64_t N = 0;
@@ -69,6 +70,7 @@ struct mgr_handle {
     int64_t *off_all = nullptr;        // [nrays*N] when stored
     int32_t *tcell = nullptr;
     double *tshift = nullptr, *tdz = nullptr;
+    MixedPoint *tmp_ = nullptr;        // mixed-format records
     int64_t tcap = 0;                  // point capacity of tcell/tshift/tdz
     int32_t *blen = nullptr;           // batch lengths [nrays*bcap]
     int64_t *boff = nullptr;           // batch offsets
@@ -117,6 +119,7 @@ void free_traces(mgr_handle *h) {
     free_ptr((void *&)h->tcell);
     free_ptr((void *&)h->tshift);
     free_ptr((void *&)h->tdz);
+    free_ptr((void *&)h->tmp_);
     free_ptr((void *&)h->blen);
     free_ptr((void *&)h->boff);
     free_ptr(h->scan_tmp);
@@ -332,6 +335,7 @@ void do_upload(mgr_handle *h, const mgr_model_desc *d) {
     m.nfreqs = h->nfreqs;
     m.ncolpar = h->ncolpar;
     m.pop_prec = d->pop_prec;
+    m.mixed_scale = h->mixed_scale;
     m.pos = upload(h, d->position, 3 * N, T);
     m.vel = upload(h, d->velocity, 3 * N, T);
     m.rays = upload(h, d->rays, 3 * (int64_t)d->nrays, T);
@@ -429,6 +433,7 @@ void ensure_scan_tmp(mgr_handle *h, int64_t n) {
 int64_t scan_lengths(mgr_handle *h, const int32_t *lens, int64_t *off, int64_t n) {
     widen_kernel<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(lens, off, n);
     ck(cudaGetLastError(), "widen");
+    h->launches += 1;
     ensure_scan_tmp(h, n);
     size_t bytes = h->scan_tmp_bytes;
     ck(cub::DeviceScan::ExclusiveSum(h->scan_tmp, bytes, off, off, n, h->stream), "scan");
@@ -445,14 +450,16 @@ void ensure_points(mgr_handle *h, int64_t npts) {
     free_ptr((void *&)h->tcell);
     free_ptr((void *&)h->tshift);
     free_ptr((void *&)h->tdz);
+    free_ptr((void *&)h->tmp_);
     const int64_t cap = std::max<int64_t>(npts, 1);
     h->tcell = dalloc<int32_t>(h, cap, nullptr);
     h->tshift = dalloc<double>(h, cap, nullptr);
     h->tdz = dalloc<double>(h, cap, nullptr);
+    h->tmp_ = dalloc<MixedPoint>(h, cap, nullptr);
     h->tcap = cap;
 }
 
-constexpr int64_t kBytesPerPoint = sizeof(int32_t) + 2 * sizeof(double);
+constexpr int64_t kBytesPerPoint = sizeof(int32_t) + 2 * sizeof(double) + sizeof(MixedPoint);
 
 int64_t default_budget(mgr_handle *h) {
     size_t fr = 0, tot = 0;
@@ -468,6 +475,7 @@ void do_trace(mgr_handle *h) {
     if (!h->len_all) h->len_all = dalloc<int32_t>(h, n, nullptr);
     reset_flags(h);
     ck(launch_trace_count(h->mv, 0, N, h->len_all, h->flags, h->stream), "trace count");
+    h->launches += 1;
     check_flags(h, "trace");
     h->h_len.resize(n);
     ck(cudaMemcpy(h->h_len.data(), h->len_all, n * sizeof(int32_t), cudaMemcpyDeviceToHost), "d2h lens");
@@ -494,9 +502,11 @@ void do_trace(mgr_handle *h) {
         h->off_all = dalloc<int64_t>(h, n, nullptr);
         const int64_t tot = scan_lengths(h, h->len_all, h->off_all, n);
         ensure_points(h, tot);
-        TraceView t{0, N, (int)R, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz};
+        TraceView t{0, N, (int)R, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
         reset_flags(h);
-        ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->flags, h->stream), "trace fill");
+        ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->tmp_, h->flags, h->stream),
+           "trace fill");
+        h->launches += 1;
         check_flags(h, "trace fill");
         h->stored = true;
         h->batch_origins = N;
@@ -535,8 +545,10 @@ TraceView build_batch(mgr_handle *h, int64_t o0, int64_t cnt) {
        "batch lens");
     const int64_t tot = scan_lengths(h, h->blen, h->boff, R * cnt);
     ensure_points(h, tot);
-    TraceView t{o0, cnt, (int)R, h->boff, h->blen, h->tcell, h->tshift, h->tdz};
-    ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->flags, h->stream), "trace fill");
+    TraceView t{o0, cnt, (int)R, h->boff, h->blen, h->tcell, h->tshift, h->tdz, h->tmp_};
+    ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->tmp_, h->flags, h->stream),
+       "trace fill");
+    h->launches += 1;
     return t;
 }
 
@@ -558,13 +570,15 @@ void do_solve(mgr_handle *h, int precision) {
     reset_flags(h);
     ck(cudaEventRecord(h->ev0, h->stream), "event");
     if (h->stored) {
-        TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz};
+        TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
         ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
+        h->launches += 1;
     } else {
         for (int64_t o0 = 0; o0 < h->N; o0 += h->batch_origins) {
             const int64_t cnt = std::min(h->batch_origins, h->N - o0);
             TraceView t = build_batch(h, o0, cnt);
             ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
+            h->launches += 1;
         }
     }
     ck(cudaEventRecord(h->ev1, h->stream), "event");
@@ -584,6 +598,7 @@ void do_stateq(mgr_handle *h) {
     need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
     reset_flags(h);
     ck(launch_stateq(h->mv, level_args(h), h->flags, h->stream), "stateq");
+    h->launches += 2;
     check_flags(h, "statistical equilibrium");
     read_stats(h);
 }
@@ -594,6 +609,7 @@ void do_ng(mgr_handle *h) {
     ck(launch_ng(h->mv, a, h->stream), "ng");
     ck(launch_convergence(h->mv, a, h->stream), "convergence");
     ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
+    h->launches += 6;
     read_stats(h);
 }
 
@@ -638,6 +654,8 @@ mgr_status mgr_create(int device, mgr_handle **out) {
         ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
         ck(cudaEventCreate(&h->ev0), "event");
         ck(cudaEventCreate(&h->ev1), "event");
+        ck(cudaEventCreate(&h->tev0), "event");
+        ck(cudaEventCreate(&h->tev1), "event");
         ck(cudaMallocHost(&h->h_stats, 8 * sizeof(double)), "pinned");
         ck(cudaMallocHost(&h->h_flags, sizeof(DevFlags)), "pinned");
     });
@@ -658,6 +676,8 @@ mgr_status mgr_destroy(mgr_handle *h) {
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->tev0) cudaEventDestroy(h->tev0);
+    if (h->tev1) cudaEventDestroy(h->tev1);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MGR_OK;
@@ -714,6 +734,7 @@ mgr_status mgr_compute_LTE_level_populations(mgr_handle *h) {
         const LevelArgs a = level_args(h);
         ck(launch_lte(h->mv, a, h->stream), "lte");
         ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
+        h->launches += 2;
         ck(cudaStreamSynchronize(h->stream), "lte sync");
         h->pops_valid = true;
     });
@@ -781,6 +802,7 @@ mgr_status mgr_compute_Jeff(mgr_handle *h) {
     return run(h, [&] {
         need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
         ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
+        h->launches += 1;
         ck(cudaStreamSynchronize(h->stream), "jeff sync");
     });
 }
@@ -820,6 +842,7 @@ mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts
             } else {
                 do_solve(h, opts->precision);
                 ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
+                h->launches += 1;
                 do_stateq(h);
                 normal++;
             }
@@ -840,6 +863,7 @@ mgr_status mgr_set_populations(mgr_handle *h, const double *pop) {
         need(h->model_loaded && pop, MGR_ERR_INVALID_ARG, "no model or NULL input");
         ck(cudaMemcpy(h->pop, pop, h->N * h->nlev * sizeof(double), cudaMemcpyHostToDevice), "h2d");
         ck(launch_emissivity_opacity(h->mv, level_args(h), h->stream), "emissivity");
+        h->launches += 1;
         ck(cudaStreamSynchronize(h->stream), "sync");
         h->pops_valid = true;
     });
@@ -898,6 +922,28 @@ mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates) {
 
 mgr_status mgr_synchronize(mgr_handle *h) {
     return run(h, [&] { ck(cudaStreamSynchronize(h->stream), "sync"); });
+}
+
+mgr_status mgr_timer_start(mgr_handle *h) {
+    return run(h, [&] { ck(cudaEventRecord(h->tev0, h->stream), "timer start"); });
+}
+
+mgr_status mgr_timer_stop(mgr_handle *h, double *ms) {
+    return run(h, [&] {
+        need(ms != nullptr, MGR_ERR_INVALID_ARG, "NULL output");
+        ck(cudaEventRecord(h->tev1, h->stream), "timer stop");
+        ck(cudaEventSynchronize(h->tev1), "timer sync");
+        float f = 0.f;
+        ck(cudaEventElapsedTime(&f, h->tev0, h->tev1), "elapsed");
+        *ms = f;
+    });
+}
+
+mgr_status mgr_get_launch_count(mgr_handle *h, int64_t *count) {
+    return run(h, [&] {
+        need(count != nullptr, MGR_ERR_INVALID_ARG, "NULL output");
+        *count = h->launches;
+    });
 }
 
 }  // extern "C"

@@ -8,7 +8,9 @@
 //   state      pop/prev1..3 [N*nlev], eps/kap [N*K] (double),
 //              Ehat/Khat [N*K] (float, scaled), Jlin/Lam/Jeff [N*K]
 //   traces     per (direction, origin): offset (int64), length (int32);
-//              points as cell (int32), shift (double), dZ (double)
+//              points as cell (int32), shift (double), dZ (double), and a
+//              16-byte record {cell, shift-1, dZ/(2X), 1/pw} in float for
+//              the mixed-precision solve (X: the float opacity scale)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -87,6 +89,15 @@ struct ModelView {
     const double *pop_tot;
     ColparDev colpar[kMaxColpar];
     double pop_prec;
+    double mixed_scale;    // X: power of two scaling the float opacities
+};
+
+// One traced point in the mixed-precision format (one 16-byte load).
+struct __align__(16) MixedPoint {
+    int32_t cell;
+    float delta;   // Doppler shift - 1
+    float dzs;     // dZ / (2 X): dtau = (chi_a + chi_b) * dzs for chi scaled by X
+    float ipw;     // 1 / profile width of the cell
 };
 
 // Trace store for one batch of origins [o_begin, o_begin + o_count).
@@ -97,6 +108,7 @@ struct TraceView {
     const int32_t *len;    // [ndir*o_count]
     const int32_t *cell;
     const double *shift, *dZ;
+    const MixedPoint *mp;  // same points, mixed format
 };
 
 // Error counters written by kernels (bounded, never trap).
@@ -113,7 +125,8 @@ struct DevFlags {
 cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_count,
                                int32_t *len, DevFlags *flags, cudaStream_t s);
 cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
-                              double *shift, double *dZ, DevFlags *flags, cudaStream_t s);
+                              double *shift, double *dZ, MixedPoint *mp, DevFlags *flags,
+                              cudaStream_t s);
 
 struct SolveArgs {
     const double *eps, *kap;        // [N*K] emissivity, opacity (FP64 path)

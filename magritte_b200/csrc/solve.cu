@@ -19,8 +19,19 @@
 //     L_oo =                                   1 / (1 + A_o F'_{o-1} + C_o G'_{o+1})
 // with F' = F/(1+F), G' = G/(1+G) the reference's F and G.  This is the same
 // linear system and the same diagonal ALO element (the reference's
-// L_diag[n_ar] = inv_C/(F + G/(1+G))), with O(1) state per lane and a single
-// division per point for the recursion.
+// L_diag[n_ar] = inv_C/(F + G/(1+G))), with O(1) state per lane.  Written
+// with p = (dtau_far + dtau_near) dtau_far / 2 and q = (...) dtau_near / 2,
+// one elimination step toward the origin is, for either half,
+//     D = 1 / (p (1 + q) + q F');  S <- (t p + S) D q;  F' <- q (p + F') D
+// i.e. one reciprocal per point, and the two halves are independent chains
+// that a lane advances together for instruction-level parallelism.
+//
+// Precision policies:
+//   FP64  every quantity in double, as the reference.
+//   MIXED opacity, emissivity, source function and optical-depth increment
+//         in float, in dimensionless form (frequency offsets in Doppler
+//         widths relative to the line, opacities scaled by a power of two
+//         X); the elimination, u, the ALO and all accumulations in double.
 //
 // Outputs per origin: the line integrals Jlin[o][k] = sum_z w_z J[o][k,z]
 // (Simulation::compute_Jeff, sim_lines.tpp:185-198) and the diagonal ALO
@@ -34,57 +45,49 @@ namespace {
 
 constexpr int kWarpsPerBlock = 4;
 
-// Per-lane frequency context of one bin at one origin.
+// 1/x for positive normal x: hardware estimate refined by two Newton-Raphson
+// steps y <- y (2 - x y) (accurate to about one ulp).
+__device__ __forceinline__ double rcp_pos(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+// Per-lane constants of one bin at one origin.
 struct BinCtx {
     double nu_o;      // bin frequency at the origin (sim_spectrum.tpp:37-41)
     int k;            // line of the bin
-    int lo, hi;       // lines whose profile window can reach this bin
+    int lo, hi;       // lines whose +-11-width window can reach this bin
+    float q;          // pw_o * root_z: offset of the bin from its line, in units of nu
 };
 
-// ---------------------------------------------------------------- FP64 path
-// Thermodynamics::profile with 1/exp(x^2) written as exp(-x^2) and
-// 1/width as (1/line)(1/pw); same function to a few ulp.
-__device__ __forceinline__ void eta_chi_fp64(const ModelView &m, const double *__restrict__ eps,
-                                             const double *__restrict__ kap, int64_t p,
-                                             double freq, const BinCtx &b, double &eta,
-                                             double &chi) {
-    eta = 0.0;
-    chi = 1.0E-26;
-    const double pwp = __ldg(m.pw + p);
-    const double ipw = __ldg(m.inv_pw + p);
-    const int K = m.nrad;
-    for (int l = b.lo; l <= b.hi; l++) {
-        const double line_l = __ldg(m.line + l);
-        const double width = line_l * pwp;
-        const double diff = freq - line_l;
-        if (diff <= 11.0 * width && diff >= -11.0 * width) {
-            const double inv_w = __ldg(m.inv_line + l) * ipw;
-            const double x = inv_w * diff;
-            const double prof = inv_w * kINVERSE_SQRT_PI * exp(-(x * x));
-            const double fp = freq * prof;
-            eta += __ldg(eps + p * K + l) * fp;
-            chi += __ldg(kap + p * K + l) * fp;
-        }
-    }
-}
+// What the boundary condition needs, passed by value to the out-of-line
+// helper below.
+struct BdyCtx {
+    const int32_t *cell2bdy;
+    const double *bdy_T, *pw, *line, *roots;
+    int nq, nf;
+};
 
 // Radiation::rescale_I_bdy (scalar build, Model/Radiation/radiation.tpp:341-373)
 // with I_bdy = planck(T_b, nu_p) evaluated on the fly.  The grid of cell p is
 // ascending, so the reference's linear notch search equals a lower bound.
-__device__ __forceinline__ double boundary_intensity(const ModelView &m, double freq, int64_t p,
-                                                     DevFlags *flags) {
-    const int b = __ldg(m.cell2bdy + p);
+__device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p, DevFlags *flags) {
+    const int b = __ldg(c.cell2bdy + p);
     if (b < 0) {
         atomicAdd(&flags->trace_err, 1ull);
         return 0.0;
     }
-    const double T = __ldg(m.bdy_T + b);
-    const double pwp = __ldg(m.pw + p);
-    const int nq = m.nquads, nf = m.nfreqs;
+    const double T = __ldg(c.bdy_T + b);
+    const double pwp = __ldg(c.pw + p);
+    const int nq = c.nq, nf = c.nf;
     auto nu_at = [&](int f) {
         const int k = f / nq;
-        const double line = __ldg(m.line + k);
-        return radd(line, rmul(rmul(line, pwp), __ldg(m.roots + (f - k * nq))));
+        const double line = __ldg(c.line + k);
+        return radd(line, rmul(rmul(line, pwp), __ldg(c.roots + (f - k * nq))));
     };
     int lo = 0, hi = nf;   // first f with freq <= nu(f), or nf
     while (lo < hi) {
@@ -92,147 +95,291 @@ __device__ __forceinline__ double boundary_intensity(const ModelView &m, double 
         if (freq <= nu_at(mid)) hi = mid;
         else lo = mid + 1;
     }
-    int notch = lo < nf ? lo : nf - 1;
+    const int notch = lo < nf ? lo : nf - 1;
     if (notch == 0 || notch == nf - 1) return planck(T, nu_at(notch));
     const double nu1 = nu_at(notch), nu2 = nu_at(notch - 1);
     const double I1 = planck(T, nu1), I2 = planck(T, nu2);
     return (I2 - I1) / (nu2 - nu1) * (freq - nu1) + I1;
 }
 
-struct Trace {
+__device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
+    BdyCtx c;
+    c.cell2bdy = m.cell2bdy;
+    c.bdy_T = m.bdy_T;
+    c.pw = m.pw;
+    c.line = m.line;
+    c.roots = m.roots;
+    c.nq = m.nquads;
+    c.nf = m.nfreqs;
+    return c;
+}
+
+// ---------------------------------------------------------------- policies
+
+struct Fp64Policy {
+    using Real = double;
+    struct Pt {
+        int cell;
+        double shift, dz;
+    };
     const int32_t *cell;
     const double *shift, *dZ;
-    int n;
+    const double *eps, *kap;
+
+    __device__ __forceinline__ Pt load(int64_t i) const {
+        Pt p;
+        p.cell = __ldg(cell + i);
+        p.shift = __ldg(shift + i);
+        p.dz = __ldg(dZ + i);
+        return p;
+    }
+    __device__ __forceinline__ double freq(const Pt &p, const BinCtx &b) const {
+        return p.shift * b.nu_o;
+    }
+    // Simulation::get_eta_and_chi (simulation.tpp:385-481) over the lines in
+    // the bin's window, with Thermodynamics::profile (thermodynamics.tpp:16-29);
+    // 1/exp(x^2) is written exp(-x^2) and 1/width (1/line)(1/pw).
+    __device__ __forceinline__ void eval(const ModelView &m, int p, double freq, const BinCtx &b,
+                                         double &chi, double &t) const {
+        double eta = 0.0;
+        chi = 1.0E-26;
+        const double pwp = __ldg(m.pw + p);
+        const double ipw = __ldg(m.inv_pw + p);
+        const int K = m.nrad;
+        for (int l = b.lo; l <= b.hi; l++) {
+            const double line_l = __ldg(m.line + l);
+            const double width = line_l * pwp;
+            const double diff = freq - line_l;
+            if (diff <= 11.0 * width && diff >= -11.0 * width) {
+                const double inv_w = __ldg(m.inv_line + l) * ipw;
+                const double x = inv_w * diff;
+                const double fp = freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x)));
+                eta += __ldg(eps + (int64_t)p * K + l) * fp;
+                chi += __ldg(kap + (int64_t)p * K + l) * fp;
+            }
+        }
+        t = eta * rcp_pos(chi);
+    }
+    __device__ __forceinline__ void eval_pt(const ModelView &m, const Pt &p, const BinCtx &b,
+                                            double &chi, double &t) const {
+        eval(m, p.cell, freq(p, b), b, chi, t);
+    }
+    __device__ __forceinline__ static double dtau(double chi_a, double chi_b, double dz) {
+        return 0.5 * (chi_a + chi_b) * dz;
+    }
+    __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
+                                           double &chi, double &t) const {
+        eval(m, o, b.nu_o, b, chi, t);
+    }
+    __device__ __forceinline__ double to_phys(double chi) const { return chi; }
 };
 
-// Forward elimination over the front half (far end first) and backward
-// elimination over the back half, meeting at the origin.
-__device__ __forceinline__ void sweep_fp64(const ModelView &m, const double *__restrict__ eps,
-                                           const double *__restrict__ kap, const BinCtx &b,
-                                           const Trace &fr, const Trace &bk, double t_o,
-                                           double chi_o, int64_t origin, DevFlags *flags,
-                                           double &u, double &L) {
-    // ---- front: positions 0 .. n_ar-1 are elements n_ar-1 .. 0
-    int j = fr.n - 1;
-    int32_t p = __ldg(fr.cell + j);
-    double freq = __ldg(fr.shift + j) * b.nu_o;
-    double eta, chi;
-    eta_chi_fp64(m, eps, kap, p, freq, b, eta, chi);
-    double chi_a = chi, t_a = eta / chi, dz_a = __ldg(fr.dZ + j);
-    const double I0 = boundary_intensity(m, freq, p, flags);
-    double Fp = 0.0, Su = 0.0, dtau_prev = 0.0;
-    for (int n = 1; n <= fr.n; n++) {
-        double chi_b, t_b, dz_b = 0.0;
-        if (n < fr.n) {
-            j = fr.n - 1 - n;
-            p = __ldg(fr.cell + j);
-            freq = __ldg(fr.shift + j) * b.nu_o;
-            eta_chi_fp64(m, eps, kap, p, freq, b, eta, chi);
-            chi_b = chi;
-            t_b = eta / chi;
-            dz_b = __ldg(fr.dZ + j);
-        } else {
-            chi_b = chi_o;
-            t_b = t_o;
+struct MixedPolicy {
+    using Real = float;
+    using Pt = MixedPoint;
+    const MixedPoint *mp;
+    const float2 *ek;         // [N*K] (eps, kap) * INVSQRTPI / pw * X
+    float floor_hat;          // 1e-26 * X
+    double inv_scale;         // 1 / X
+    const double *eps, *kap;  // for lines other than the bin's own
+
+    __device__ __forceinline__ Pt load(int64_t i) const {
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(mp) + i);
+        Pt p;
+        p.cell = __float_as_int(v.x);
+        p.delta = v.y;
+        p.dzs = v.z;
+        p.ipw = v.w;
+        return p;
+    }
+    __device__ __forceinline__ double freq(const Pt &p, const BinCtx &b) const {
+        return (1.0 + (double)p.delta) * b.nu_o;
+    }
+    // Scaled opacity and source function.  For the bin's own line,
+    // x = ((1+delta)(1+q) - 1) / pw_p and nu/line = (1+delta)(1+q), so
+    // chi X = 1e-26 X + Khat (nu/line) exp(-x^2); other lines in the window
+    // (overlapping profiles) are added from the double tables.
+    __device__ __forceinline__ void eval_pt(const ModelView &m, const Pt &p, const BinCtx &b,
+                                            float &chi, float &t) const {
+        const float off = fmaf(p.delta, b.q, p.delta + b.q);   // (1+d)(1+q) - 1
+        const float x = off * p.ipw;
+        const float r = 1.0f + off;
+        const int K = m.nrad;
+        float eta = 0.0f;
+        chi = floor_hat;
+        if (fabsf(x) <= 11.0f) {
+            const float2 e = __ldg(ek + (int64_t)p.cell * K + b.k);
+            const float g = r * __expf(-x * x);
+            eta = e.x * g;
+            chi = fmaf(e.y, g, chi);
         }
-        const double dtau = 0.5 * (chi_a + chi_b) * dz_a;
-        if (n == 1) {
-            // row 0: B0 = 1 + 2/dtau + 2/dtau^2, S0 = t + 2 I0/dtau
-            const double D = 1.0 / (dtau * dtau + 2.0 * dtau + 2.0);
-            Fp = (dtau * dtau + 2.0 * dtau) * D;
-            Su = (t_a * dtau * dtau + 2.0 * I0 * dtau) * D;
-        } else {
-            const double h = 0.5 * (dtau_prev + dtau);
-            const double invA = h * dtau_prev, invC = h * dtau;
-            const double D = 1.0 / (invA * (1.0 + invC) + invC * Fp);
-            const double Su_new = (t_a * invA + Su) * D * invC;
-            Fp = invC * (invA + Fp) * D;
-            Su = Su_new;
+        if (b.lo != b.hi) {
+            const double fr = freq(p, b);
+            const double pwp = __ldg(m.pw + p.cell);
+            const double ipw = __ldg(m.inv_pw + p.cell);
+            double ea = 0.0, ca = 0.0;
+            for (int l = b.lo; l <= b.hi; l++) {
+                if (l == b.k) continue;
+                const double line_l = __ldg(m.line + l);
+                const double width = line_l * pwp;
+                const double diff = fr - line_l;
+                if (diff <= 11.0 * width && diff >= -11.0 * width) {
+                    const double inv_w = __ldg(m.inv_line + l) * ipw;
+                    const double xx = inv_w * diff;
+                    const double fp = fr * (inv_w * kINVERSE_SQRT_PI * exp(-(xx * xx)));
+                    ea += __ldg(eps + (int64_t)p.cell * K + l) * fp;
+                    ca += __ldg(kap + (int64_t)p.cell * K + l) * fp;
+                }
+            }
+            eta += (float)(ea * m.mixed_scale);
+            chi += (float)(ca * m.mixed_scale);
         }
-        dtau_prev = dtau;
+        t = __fdividef(eta, chi);
+    }
+    __device__ __forceinline__ static double dtau(float chi_a, float chi_b, float dzs) {
+        return (double)((chi_a + chi_b) * dzs);
+    }
+    __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
+                                           float &chi, float &t) const {
+        Pt p;
+        p.cell = o;
+        p.delta = 0.0f;
+        p.dzs = 0.0f;
+        p.ipw = (float)__ldg(m.inv_pw + o);
+        eval_pt(m, p, b, chi, t);
+    }
+    __device__ __forceinline__ double to_phys(float chi) const { return (double)chi * inv_scale; }
+};
+
+// ------------------------------------------------------------------ chains
+
+// Elimination of one half of the ray pair from its far end toward the origin.
+template <class Pol>
+struct Chain {
+    using Real = typename Pol::Real;
+    Real chi_a, t_a;      // current point
+    Real dz_a;            // its increment toward the origin (policy units)
+    double F, S, dtau_prev;
+
+    // row of the far end (boundary row: B = 1 + 2/dtau + 2/dtau^2,
+    // S = t + 2 I/dtau)
+    __device__ __forceinline__ void first(Real chi_b, Real t_b, Real dz_b, double I) {
+        const double d = Pol::dtau(chi_a, chi_b, dz_a);
+        const double D = rcp_pos(fma(d, d + 2.0, 2.0));
+        F = d * (d + 2.0) * D;
+        S = fma((double)t_a * d, d, 2.0 * I * d) * D;
+        dtau_prev = d;
         chi_a = chi_b;
         t_a = t_b;
         dz_a = dz_b;
     }
-    const double dtau_front = dtau_prev;   // dtau[o-1]
+    __device__ __forceinline__ void step(Real chi_b, Real t_b, Real dz_b) {
+        const double d = Pol::dtau(chi_a, chi_b, dz_a);
+        const double h = 0.5 * (dtau_prev + d);
+        const double p = h * dtau_prev, q = h * d;
+        const double D = rcp_pos(fma(p, 1.0 + q, q * F));
+        S = fma((double)t_a, p, S) * D * q;
+        F = q * (p + F) * D;
+        dtau_prev = d;
+        chi_a = chi_b;
+        t_a = t_b;
+        dz_a = dz_b;
+    }
+};
 
-    if (bk.n == 0) {
-        // the origin is the last row: S_d = t + 2 I_n / dtau with the
-        // origin's own boundary value at this bin (simulation.tpp:343-348)
+template <class Pol>
+__device__ __forceinline__ typename Pol::Real dz_of(const typename Pol::Pt &p);
+template <>
+__device__ __forceinline__ double dz_of<Fp64Policy>(const Fp64Policy::Pt &p) { return p.dz; }
+template <>
+__device__ __forceinline__ float dz_of<MixedPolicy>(const MixedPolicy::Pt &p) { return p.dzs; }
+
+template <class Pol>
+__device__ __forceinline__ int cell_of(const typename Pol::Pt &p) { return p.cell; }
+
+// u and L at the origin for one ray pair.
+template <class Pol>
+__device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const BinCtx &b,
+                                      int64_t ofr, int nfr, int64_t obk, int nbk,
+                                      typename Pol::Real chi_o, typename Pol::Real t_o,
+                                      int origin, DevFlags *flags, double &u, double &L) {
+    using Real = typename Pol::Real;
+    Chain<Pol> fr, bk;
+    Real chi, t;
+    const BdyCtx bc = bdy_ctx(m);
+    // far ends
+    double I0;
+    {
+        const auto p = pol.load(ofr + nfr - 1);
+        pol.eval_pt(m, p, b, chi, t);
+        fr.chi_a = chi; fr.t_a = t; fr.dz_a = dz_of<Pol>(p);
+        I0 = boundary_intensity(bc, pol.freq(p, b), cell_of<Pol>(p), flags);
+    }
+    double In = 0.0;
+    if (nbk > 0) {
+        const auto p = pol.load(obk + nbk - 1);
+        pol.eval_pt(m, p, b, chi, t);
+        bk.chi_a = chi; bk.t_a = t; bk.dz_a = dz_of<Pol>(p);
+        In = boundary_intensity(bc, pol.freq(p, b), cell_of<Pol>(p), flags);
+    } else {
         const int bo = __ldg(m.cell2bdy + origin);
-        double In = 0.0;
         if (bo >= 0) In = planck(__ldg(m.bdy_T + bo), b.nu_o);
         else atomicAdd(&flags->trace_err, 1ull);
-        const double d = dtau_front;
-        const double den = 1.0 / (d * d + 2.0 * d + 2.0 * Fp);
-        u = (t_o * d * d + 2.0 * In * d + 2.0 * Su) * den;
+    }
+    // both halves advance together; the front is never shorter
+    for (int s = 1; s <= nfr; s++) {
+        Real chi_b, t_b, dz_b = Real(0);
+        if (s < nfr) {
+            const auto p = pol.load(ofr + nfr - 1 - s);
+            pol.eval_pt(m, p, b, chi_b, t_b);
+            dz_b = dz_of<Pol>(p);
+        } else {
+            chi_b = chi_o;
+            t_b = t_o;
+        }
+        if (s == 1) fr.first(chi_b, t_b, dz_b, I0);
+        else fr.step(chi_b, t_b, dz_b);
+        if (s <= nbk) {
+            Real chi_c, t_c, dz_c = Real(0);
+            if (s < nbk) {
+                const auto p = pol.load(obk + nbk - 1 - s);
+                pol.eval_pt(m, p, b, chi_c, t_c);
+                dz_c = dz_of<Pol>(p);
+            } else {
+                chi_c = chi_o;
+                t_c = t_o;
+            }
+            if (s == 1) bk.first(chi_c, t_c, dz_c, In);
+            else bk.step(chi_c, t_c, dz_c);
+        }
+    }
+    const double to = (double)t_o;
+    if (nbk == 0) {
+        // the origin is the last row: S_d = t + 2 I_n / dtau
+        const double d = fr.dtau_prev;
+        const double den = rcp_pos(fma(d, d + 2.0, 2.0 * fr.F));
+        u = fma(to * d, d, fma(2.0 * In, d, 2.0 * fr.S)) * den;
         L = d * d * den;
         return;
     }
-
-    // ---- back: positions last .. o+1 are elements n_r-1 .. 0
-    j = bk.n - 1;
-    p = __ldg(bk.cell + j);
-    freq = __ldg(bk.shift + j) * b.nu_o;
-    eta_chi_fp64(m, eps, kap, p, freq, b, eta, chi);
-    chi_a = chi;
-    t_a = eta / chi;
-    dz_a = __ldg(bk.dZ + j);
-    const double In = boundary_intensity(m, freq, p, flags);
-    double Gp = 0.0, Sb = 0.0;
-    dtau_prev = 0.0;
-    for (int n = 1; n <= bk.n; n++) {
-        double chi_b, t_b, dz_b = 0.0;
-        if (n < bk.n) {
-            j = bk.n - 1 - n;
-            p = __ldg(bk.cell + j);
-            freq = __ldg(bk.shift + j) * b.nu_o;
-            eta_chi_fp64(m, eps, kap, p, freq, b, eta, chi);
-            chi_b = chi;
-            t_b = eta / chi;
-            dz_b = __ldg(bk.dZ + j);
-        } else {
-            chi_b = chi_o;
-            t_b = t_o;
-        }
-        const double dtau = 0.5 * (chi_a + chi_b) * dz_a;
-        if (n == 1) {
-            const double D = 1.0 / (dtau * dtau + 2.0 * dtau + 2.0);
-            Gp = (dtau * dtau + 2.0 * dtau) * D;
-            Sb = (t_a * dtau * dtau + 2.0 * In * dtau) * D;
-        } else {
-            // backward row: A uses the step toward the origin (dtau),
-            // C the step toward the far end (dtau_prev)
-            const double h = 0.5 * (dtau_prev + dtau);
-            const double invA = h * dtau, invC = h * dtau_prev;
-            const double D = 1.0 / (invC * (1.0 + invA) + invA * Gp);
-            const double Sb_new = (t_a * invC + Sb) * D * invA;
-            Gp = invA * (invC + Gp) * D;
-            Sb = Sb_new;
-        }
-        dtau_prev = dtau;
-        chi_a = chi_b;
-        t_a = t_b;
-        dz_a = dz_b;
-    }
-    const double dtau_back = dtau_prev;   // dtau[o]
-
-    // ---- origin row
-    const double h = 0.5 * (dtau_front + dtau_back);
-    const double invA = h * dtau_front, invC = h * dtau_back;
-    const double invAC = invA * invC;
-    const double den = 1.0 / (invAC + Fp * invC + Gp * invA);
-    u = (t_o * invAC + Su * invC + Sb * invA) * den;
-    L = invAC * den;
+    // origin row: A_o from the front step, C_o from the back step
+    const double h = 0.5 * (fr.dtau_prev + bk.dtau_prev);
+    const double iA = h * fr.dtau_prev, iC = h * bk.dtau_prev;
+    const double iAC = iA * iC;
+    const double den = rcp_pos(fma(fr.F, iC, fma(bk.F, iA, iAC)));
+    u = fma(to, iAC, fma(fr.S, iC, bk.S * iA)) * den;
+    L = iAC * den;
 }
 
+template <class Pol>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    formal_solve_fp64_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
+    formal_solve_kernel(ModelView m, TraceView t, SolveArgs a, Pol pol, DevFlags *flags) {
+    using Real = typename Pol::Real;
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
     if (oi >= t.o_count) return;
-    const int64_t o = t.o_begin + oi;
+    const int o = (int)(t.o_begin + oi);
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
     double *sJ = smem + (size_t)warp * 2 * K;
     double *sL = sJ + K;
@@ -251,19 +398,20 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         b.lo = m.win_lo[b.k];
         b.hi = m.win_hi[b.k];
         const double line_k = m.line[b.k];
-        b.nu_o = radd(line_k, rmul(rmul(line_k, pw_o), m.roots[z]));
+        const double root = m.roots[z];
+        b.nu_o = radd(line_k, rmul(rmul(line_k, pw_o), root));
+        b.q = (float)(pw_o * root);
 
         // origin: same opacity and source for every pair
-        double eta_o, chi_o;
-        eta_chi_fp64(m, a.eps, a.kap, o, b.nu_o, b, eta_o, chi_o);
-        const double t_o = eta_o / chi_o;
+        Real chi_o, t_o;
+        pol.origin(m, o, b, chi_o, t_o);
         // ALO factor without the pair weight (raypair_lambda.tpp:26-29, :115-121)
         const double width_o = line_k * pw_o;
-        const double d_o = b.nu_o - line_k;
         const double iw = 1.0 / width_o;
-        const double xo = iw * d_o;
+        const double xo = iw * (b.nu_o - line_k);
         const double prof_o = iw * kINVERSE_SQRT_PI * exp(-(xo * xo));
-        const double lam_pre = m.A[b.k] * (m.qw[z] * 2.0) * (b.nu_o * prof_o / chi_o);
+        const double chi_o_d = pol.to_phys(chi_o);
+        const double lam_pre = m.A[b.k] * (m.qw[z] * 2.0) * (b.nu_o * prof_o / chi_o_d);
 
         double Jf = 0.0, Lf = 0.0;
         for (int r = 0; r < m.npairs; r++) {
@@ -274,14 +422,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
             const int nr_ = t.len[ir], nar_ = t.len[iar];
             // the longer trace is the front half (sim_radiation.tpp:164-171)
             const bool rfront = nr_ > nar_;
-            Trace fr, bk;
             const int64_t ofr = rfront ? t.off[ir] : t.off[iar];
             const int64_t obk = rfront ? t.off[iar] : t.off[ir];
-            fr.n = rfront ? nr_ : nar_;
-            bk.n = rfront ? nar_ : nr_;
-            fr.cell = t.cell + ofr; fr.shift = t.shift + ofr; fr.dZ = t.dZ + ofr;
-            bk.cell = t.cell + obk; bk.shift = t.shift + obk; bk.dZ = t.dZ + obk;
-            if (fr.n == 0) {
+            const int nfr = rfront ? nr_ : nar_;
+            const int nbk = rfront ? nar_ : nr_;
+            if (nfr == 0) {
                 // only the origin on the ray pair: J += 2 w I_bdy (sim_radiation.tpp:243-264)
                 const int bo = m.cell2bdy[o];
                 double I = 0.0;
@@ -291,11 +436,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                 continue;
             }
             double u, L;
-            sweep_fp64(m, a.eps, a.kap, b, fr, bk, t_o, chi_o, o, flags, u, L);
+            sweep<Pol>(m, pol, b, ofr, nfr, obk, nbk, chi_o, t_o, o, flags, u, L);
             Jf += 2.0 * wr * u;
             Lf += lam_pre * wr * L;
         }
-        if (a.J && active) a.J[o * nf + f] = Jf;
+        if (a.J && active) a.J[(int64_t)o * nf + f] = Jf;
 
         // line integrals over the bins of this chunk
         const double jw = active ? m.qw[z] * Jf : 0.0;
@@ -315,8 +460,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
         __syncwarp();
     }
     for (int k = lane; k < K; k += 32) {
-        a.Jlin[o * K + k] = sJ[k];
-        a.Lam[o * K + k] = sL[k];
+        a.Jlin[(int64_t)o * K + k] = sJ[k];
+        a.Lam[(int64_t)o * K + k] = sL[k];
     }
 }
 
@@ -327,8 +472,26 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
     if (t.o_count == 0) return cudaSuccess;
     const int64_t blocks = (t.o_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const size_t shmem = (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
-    (void)precision;
-    formal_solve_fp64_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, flags);
+    if (precision == MGR_MIXED) {
+        MixedPolicy pol;
+        pol.mp = t.mp;
+        pol.ek = a.ehat_khat;
+        pol.floor_hat = (float)(1.0E-26 * a.mixed_scale);
+        pol.inv_scale = 1.0 / a.mixed_scale;
+        pol.eps = a.eps;
+        pol.kap = a.kap;
+        formal_solve_kernel<MixedPolicy>
+            <<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, pol, flags);
+    } else {
+        Fp64Policy pol;
+        pol.cell = t.cell;
+        pol.shift = t.shift;
+        pol.dZ = t.dZ;
+        pol.eps = a.eps;
+        pol.kap = a.kap;
+        formal_solve_kernel<Fp64Policy>
+            <<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, pol, flags);
+    }
     return cudaGetLastError();
 }
 

@@ -72,17 +72,27 @@ struct CountSink {
     __device__ __forceinline__ void push(int64_t, double, double) { n++; }
 };
 
-// Sink that writes points into the slot [base, base+cap).
+// Sink that writes points into the slot [base, base+cap), in both the
+// double format and the 16-byte mixed-precision record.
 struct WriteSink {
     int64_t n = 0, cap, base;
     int32_t *cell;
     double *shift, *dZ;
+    MixedPoint *mp;
+    const double *inv_pw;
+    double half_inv_scale;
     bool over = false;
     __device__ __forceinline__ void push(int64_t c, double s, double z) {
         if (n < cap) {
             cell[base + n] = (int32_t)c;
             shift[base + n] = s;
             dZ[base + n] = z;
+            MixedPoint q;
+            q.cell = (int32_t)c;
+            q.delta = (float)(s - 1.0);
+            q.dzs = (float)(z * half_inv_scale);
+            q.ipw = (float)inv_pw[c];
+            mp[base + n] = q;
         } else {
             over = true;
         }
@@ -100,7 +110,7 @@ __device__ __forceinline__ bool set_data(int64_t crt, int64_t nxt, double shift_
     const double dshift_abs = fabs(dshift);
     if (dshift_abs > dshift_max) {
         const double q = radd(rdiv(dshift_abs, dshift_max), 1.0);
-        if (!(q <= 10000.5)) return false;          // also catches NaN
+        if (!(q < 10001.0)) return false;           // n_interpl > 10000, or NaN
         const long long n_interpl = (long long)q;
         const long long half_n_interpl = (long long)rmul(0.5, (double)n_interpl);
         const double dZ_interpl = rdiv(dZ_loc, (double)n_interpl);
@@ -165,7 +175,8 @@ __global__ void __launch_bounds__(128) trace_count_kernel(ModelView m, int64_t o
 
 __global__ void __launch_bounds__(128) trace_fill_kernel(ModelView m, TraceView t,
                                                          int32_t *cell, double *shift,
-                                                         double *dZ, DevFlags *flags) {
+                                                         double *dZ, MixedPoint *mp,
+                                                         DevFlags *flags) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t total = (int64_t)t.ndir * t.o_count;
     if (idx >= total) return;
@@ -177,6 +188,9 @@ __global__ void __launch_bounds__(128) trace_fill_kernel(ModelView m, TraceView 
     sink.cell = cell;
     sink.shift = shift;
     sink.dZ = dZ;
+    sink.mp = mp;
+    sink.inv_pw = m.inv_pw;
+    sink.half_inv_scale = 0.5 / m.mixed_scale;
     const int code = walk(m, o, d, sink);
     if (code) count_error(flags, code);
     if (sink.over || (code == 0 && sink.n != sink.cap)) atomicAdd(&flags->cap_err, 1ull);
@@ -195,12 +209,13 @@ cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_co
 }
 
 cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
-                              double *shift, double *dZ, DevFlags *flags, cudaStream_t s) {
+                              double *shift, double *dZ, MixedPoint *mp, DevFlags *flags,
+                              cudaStream_t s) {
     const int64_t total = (int64_t)t.ndir * t.o_count;
     if (total == 0) return cudaSuccess;
     const int threads = 128;
     const int64_t blocks = (total + threads - 1) / threads;
-    trace_fill_kernel<<<(unsigned)blocks, threads, 0, s>>>(m, t, cell, shift, dZ, flags);
+    trace_fill_kernel<<<(unsigned)blocks, threads, 0, s>>>(m, t, cell, shift, dZ, mp, flags);
     return cudaGetLastError();
 }
 

@@ -206,6 +206,19 @@ class Simulation:
         self.error_mean.append(r)
         self.error_max.append(x)
 
+    def timer_start(self):
+        self._ck(self._lib.mgr_timer_start(self._h))
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        self._ck(self._lib.mgr_timer_stop(self._h, C.byref(ms)))
+        return ms.value
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        self._ck(self._lib.mgr_get_launch_count(self._h, C.byref(n)))
+        return n.value
+
     def solve_stats(self):
         ms, up = C.c_double(), C.c_double()
         self._ck(self._lib.mgr_get_solve_stats(self._h, C.byref(ms), C.byref(up)))

@@ -148,3 +148,27 @@ def test_errors_are_status_codes(gpu):
     with pytest.raises(MagritteError) as e:
         sim.trace()
     assert e.value.status == 2
+
+
+@pytest.mark.parametrize("make", [M.config1, lambda: small_wind(10, 5, 7), M.config3,
+                                  lambda: M.wind_model(9, seed=3, nlev=4, nside=2, vmax=40e3)])
+def test_radiation_field_mixed(gpu, make):
+    """Mixed precision against the FP64 oracle: J, Jlin and the ALO to 1e-4."""
+    model = make()
+    sim, orc = setup_pair(model, keep_J=False)
+    sim.compute_radiation_field("mixed", keep_J=True)
+    orc.compute_radiation_field()
+    orc.compute_Jeff()
+    assert rel_err(sim.J, orc.J) < MIXED_RTOL
+    assert rel_err(sim.Jlin, orc.Jlin) < MIXED_RTOL
+    assert rel_err(sim.Lambda, orc.Ls) < MIXED_RTOL
+
+
+def test_ali_mixed_populations(gpu):
+    """Converged populations in mixed precision against the FP64 oracle."""
+    model = M.lattice_cloud(10, name="lattice10")
+    sim, orc = setup_pair(model, keep_J=False)
+    sim.compute_level_populations(True, 300, "mixed", tol_max_rel=1e-7)
+    assert sim.converged
+    orc.compute_level_populations(True, 300, 1e-7)
+    assert rel_err(sim.population, orc.pop) < MIXED_RTOL
