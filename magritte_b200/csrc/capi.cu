@@ -336,6 +336,8 @@ void do_upload(mgr_handle *h, const mgr_model_desc *d) {
     m.ncolpar = h->ncolpar;
     m.pop_prec = d->pop_prec;
     m.mixed_scale = h->mixed_scale;
+    m.overlap = 0;
+    for (int k = 0; k < d->nrad; k++) m.overlap |= (wlo[k] != whi[k]);
     m.pos = upload(h, d->position, 3 * N, T);
     m.vel = upload(h, d->velocity, 3 * N, T);
     m.rays = upload(h, d->rays, 3 * (int64_t)d->nrays, T);

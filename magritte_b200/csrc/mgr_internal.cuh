@@ -90,6 +90,7 @@ struct ModelView {
     ColparDev colpar[kMaxColpar];
     double pop_prec;
     double mixed_scale;    // X: power of two scaling the float opacities
+    int overlap;           // some line window holds more than its own line
 };
 
 // One traced point in the mixed-precision format (one 16-byte load).

@@ -44,6 +44,7 @@ namespace mgr {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
+constexpr int kMinBlocks = 6;   // 24 warps per SM: at most 80 registers per thread
 
 // 1/x for positive normal x: hardware estimate refined by two Newton-Raphson
 // steps y <- y (2 - x y) (accurate to about one ulp).
@@ -116,6 +117,7 @@ __device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
 
 // ---------------------------------------------------------------- policies
 
+template <bool kOverlap>
 struct Fp64Policy {
     using Real = double;
     struct Pt {
@@ -138,7 +140,8 @@ struct Fp64Policy {
     }
     // Simulation::get_eta_and_chi (simulation.tpp:385-481) over the lines in
     // the bin's window, with Thermodynamics::profile (thermodynamics.tpp:16-29);
-    // 1/exp(x^2) is written exp(-x^2) and 1/width (1/line)(1/pw).
+    // 1/exp(x^2) is written exp(-x^2) and 1/width (1/line)(1/pw).  Without
+    // overlapping profiles the window holds the bin's own line only.
     __device__ __forceinline__ void eval(const ModelView &m, int p, double freq, const BinCtx &b,
                                          double &chi, double &t) const {
         double eta = 0.0;
@@ -146,17 +149,17 @@ struct Fp64Policy {
         const double pwp = __ldg(m.pw + p);
         const double ipw = __ldg(m.inv_pw + p);
         const int K = m.nrad;
-        for (int l = b.lo; l <= b.hi; l++) {
+        const int lo = kOverlap ? b.lo : b.k, hi = kOverlap ? b.hi : b.k;
+        for (int l = lo; l <= hi; l++) {
             const double line_l = __ldg(m.line + l);
             const double width = line_l * pwp;
             const double diff = freq - line_l;
-            if (diff <= 11.0 * width && diff >= -11.0 * width) {
-                const double inv_w = __ldg(m.inv_line + l) * ipw;
-                const double x = inv_w * diff;
-                const double fp = freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x)));
-                eta += __ldg(eps + (int64_t)p * K + l) * fp;
-                chi += __ldg(kap + (int64_t)p * K + l) * fp;
-            }
+            const bool in = diff <= 11.0 * width && diff >= -11.0 * width;
+            const double inv_w = __ldg(m.inv_line + l) * ipw;
+            const double x = inv_w * diff;
+            const double fp = in ? freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x))) : 0.0;
+            eta += __ldg(eps + (unsigned)p * K + l) * fp;
+            chi += __ldg(kap + (unsigned)p * K + l) * fp;
         }
         t = eta * rcp_pos(chi);
     }
@@ -167,6 +170,7 @@ struct Fp64Policy {
     __device__ __forceinline__ static double dtau(double chi_a, double chi_b, double dz) {
         return 0.5 * (chi_a + chi_b) * dz;
     }
+    __device__ __forceinline__ static double dz_of(const Pt &p) { return p.dz; }
     __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
                                            double &chi, double &t) const {
         eval(m, o, b.nu_o, b, chi, t);
@@ -174,6 +178,7 @@ struct Fp64Policy {
     __device__ __forceinline__ double to_phys(double chi) const { return chi; }
 };
 
+template <bool kOverlap>
 struct MixedPolicy {
     using Real = float;
     using Pt = MixedPoint;
@@ -197,23 +202,20 @@ struct MixedPolicy {
     }
     // Scaled opacity and source function.  For the bin's own line,
     // x = ((1+delta)(1+q) - 1) / pw_p and nu/line = (1+delta)(1+q), so
-    // chi X = 1e-26 X + Khat (nu/line) exp(-x^2); other lines in the window
-    // (overlapping profiles) are added from the double tables.
+    // chi X = 1e-26 X + Khat (nu/line) exp(-x^2), zero outside +-11 widths;
+    // other lines in the window (overlapping profiles) come from the double
+    // tables.
     __device__ __forceinline__ void eval_pt(const ModelView &m, const Pt &p, const BinCtx &b,
                                             float &chi, float &t) const {
         const float off = fmaf(p.delta, b.q, p.delta + b.q);   // (1+d)(1+q) - 1
         const float x = off * p.ipw;
         const float r = 1.0f + off;
         const int K = m.nrad;
-        float eta = 0.0f;
-        chi = floor_hat;
-        if (fabsf(x) <= 11.0f) {
-            const float2 e = __ldg(ek + (int64_t)p.cell * K + b.k);
-            const float g = r * __expf(-x * x);
-            eta = e.x * g;
-            chi = fmaf(e.y, g, chi);
-        }
-        if (b.lo != b.hi) {
+        const float2 e = __ldg(ek + (unsigned)p.cell * K + b.k);
+        const float g = fabsf(x) <= 11.0f ? r * __expf(-x * x) : 0.0f;
+        float eta = e.x * g;
+        chi = fmaf(e.y, g, floor_hat);
+        if (kOverlap && b.lo != b.hi) {
             const double fr = freq(p, b);
             const double pwp = __ldg(m.pw + p.cell);
             const double ipw = __ldg(m.inv_pw + p.cell);
@@ -227,8 +229,8 @@ struct MixedPolicy {
                     const double inv_w = __ldg(m.inv_line + l) * ipw;
                     const double xx = inv_w * diff;
                     const double fp = fr * (inv_w * kINVERSE_SQRT_PI * exp(-(xx * xx)));
-                    ea += __ldg(eps + (int64_t)p.cell * K + l) * fp;
-                    ca += __ldg(kap + (int64_t)p.cell * K + l) * fp;
+                    ea += __ldg(eps + (unsigned)p.cell * K + l) * fp;
+                    ca += __ldg(kap + (unsigned)p.cell * K + l) * fp;
                 }
             }
             eta += (float)(ea * m.mixed_scale);
@@ -239,6 +241,7 @@ struct MixedPolicy {
     __device__ __forceinline__ static double dtau(float chi_a, float chi_b, float dzs) {
         return (double)((chi_a + chi_b) * dzs);
     }
+    __device__ __forceinline__ static float dz_of(const Pt &p) { return p.dzs; }
     __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
                                            float &chi, float &t) const {
         Pt p;
@@ -287,17 +290,9 @@ struct Chain {
     }
 };
 
-template <class Pol>
-__device__ __forceinline__ typename Pol::Real dz_of(const typename Pol::Pt &p);
-template <>
-__device__ __forceinline__ double dz_of<Fp64Policy>(const Fp64Policy::Pt &p) { return p.dz; }
-template <>
-__device__ __forceinline__ float dz_of<MixedPolicy>(const MixedPolicy::Pt &p) { return p.dzs; }
-
-template <class Pol>
-__device__ __forceinline__ int cell_of(const typename Pol::Pt &p) { return p.cell; }
-
-// u and L at the origin for one ray pair.
+// u and L at the origin for one ray pair.  The front half has nfr >= 1
+// points (far end first at index nfr-1), the back half nbk >= 0; both are
+// eliminated toward the origin in lock step while both have points left.
 template <class Pol>
 __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const BinCtx &b,
                                       int64_t ofr, int nfr, int64_t obk, int nbk,
@@ -305,54 +300,61 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
                                       int origin, DevFlags *flags, double &u, double &L) {
     using Real = typename Pol::Real;
     Chain<Pol> fr, bk;
-    Real chi, t;
     const BdyCtx bc = bdy_ctx(m);
-    // far ends
+    Real chi, t;
+    // front: far end, boundary value, first (boundary-row) step
     double I0;
     {
         const auto p = pol.load(ofr + nfr - 1);
         pol.eval_pt(m, p, b, chi, t);
-        fr.chi_a = chi; fr.t_a = t; fr.dz_a = dz_of<Pol>(p);
-        I0 = boundary_intensity(bc, pol.freq(p, b), cell_of<Pol>(p), flags);
+        fr.chi_a = chi; fr.t_a = t; fr.dz_a = Pol::dz_of(p);
+        I0 = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
+    }
+    if (nfr >= 2) {
+        const auto p = pol.load(ofr + nfr - 2);
+        pol.eval_pt(m, p, b, chi, t);
+        fr.first(chi, t, Pol::dz_of(p), I0);
+    } else {
+        fr.first(chi_o, t_o, Real(0), I0);
     }
     double In = 0.0;
     if (nbk > 0) {
         const auto p = pol.load(obk + nbk - 1);
         pol.eval_pt(m, p, b, chi, t);
-        bk.chi_a = chi; bk.t_a = t; bk.dz_a = dz_of<Pol>(p);
-        In = boundary_intensity(bc, pol.freq(p, b), cell_of<Pol>(p), flags);
+        bk.chi_a = chi; bk.t_a = t; bk.dz_a = Pol::dz_of(p);
+        In = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
+        if (nbk >= 2) {
+            const auto q = pol.load(obk + nbk - 2);
+            pol.eval_pt(m, q, b, chi, t);
+            bk.first(chi, t, Pol::dz_of(q), In);
+        } else {
+            bk.first(chi_o, t_o, Real(0), In);
+        }
     } else {
         const int bo = __ldg(m.cell2bdy + origin);
         if (bo >= 0) In = planck(__ldg(m.bdy_T + bo), b.nu_o);
         else atomicAdd(&flags->trace_err, 1ull);
     }
-    // both halves advance together; the front is never shorter
-    for (int s = 1; s <= nfr; s++) {
-        Real chi_b, t_b, dz_b = Real(0);
-        if (s < nfr) {
-            const auto p = pol.load(ofr + nfr - 1 - s);
-            pol.eval_pt(m, p, b, chi_b, t_b);
-            dz_b = dz_of<Pol>(p);
-        } else {
-            chi_b = chi_o;
-            t_b = t_o;
-        }
-        if (s == 1) fr.first(chi_b, t_b, dz_b, I0);
-        else fr.step(chi_b, t_b, dz_b);
-        if (s <= nbk) {
-            Real chi_c, t_c, dz_c = Real(0);
-            if (s < nbk) {
-                const auto p = pol.load(obk + nbk - 1 - s);
-                pol.eval_pt(m, p, b, chi_c, t_c);
-                dz_c = dz_of<Pol>(p);
-            } else {
-                chi_c = chi_o;
-                t_c = t_o;
-            }
-            if (s == 1) bk.first(chi_c, t_c, dz_c, In);
-            else bk.step(chi_c, t_c, dz_c);
-        }
+    // both halves have interior points
+    int s = 2;
+    for (; s < nbk; s++) {
+        const auto p = pol.load(ofr + nfr - 1 - s);
+        const auto q = pol.load(obk + nbk - 1 - s);
+        Real chi_p, t_p, chi_q, t_q;
+        pol.eval_pt(m, p, b, chi_p, t_p);
+        pol.eval_pt(m, q, b, chi_q, t_q);
+        fr.step(chi_p, t_p, Pol::dz_of(p));
+        bk.step(chi_q, t_q, Pol::dz_of(q));
     }
+    if (nbk >= 2) bk.step(chi_o, t_o, Real(0));
+    // the rest of the front half
+    for (; s < nfr; s++) {
+        const auto p = pol.load(ofr + nfr - 1 - s);
+        pol.eval_pt(m, p, b, chi, t);
+        fr.step(chi, t, Pol::dz_of(p));
+    }
+    if (nfr >= 2) fr.step(chi_o, t_o, Real(0));
+
     const double to = (double)t_o;
     if (nbk == 0) {
         // the origin is the last row: S_d = t + 2 I_n / dtau
@@ -372,7 +374,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
 }
 
 template <class Pol>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     formal_solve_kernel(ModelView m, TraceView t, SolveArgs a, Pol pol, DevFlags *flags) {
     using Real = typename Pol::Real;
     extern __shared__ double smem[];
@@ -472,25 +474,33 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
     if (t.o_count == 0) return cudaSuccess;
     const int64_t blocks = (t.o_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const size_t shmem = (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
-    if (precision == MGR_MIXED) {
-        MixedPolicy pol;
+    auto run = [&](auto pol) {
+        formal_solve_kernel<decltype(pol)>
+            <<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, pol, flags);
+    };
+    auto mixed = [&](auto pol) {
         pol.mp = t.mp;
         pol.ek = a.ehat_khat;
         pol.floor_hat = (float)(1.0E-26 * a.mixed_scale);
         pol.inv_scale = 1.0 / a.mixed_scale;
         pol.eps = a.eps;
         pol.kap = a.kap;
-        formal_solve_kernel<MixedPolicy>
-            <<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, pol, flags);
-    } else {
-        Fp64Policy pol;
+        run(pol);
+    };
+    auto fp64 = [&](auto pol) {
         pol.cell = t.cell;
         pol.shift = t.shift;
         pol.dZ = t.dZ;
         pol.eps = a.eps;
         pol.kap = a.kap;
-        formal_solve_kernel<Fp64Policy>
-            <<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, pol, flags);
+        run(pol);
+    };
+    if (precision == MGR_MIXED) {
+        if (m.overlap) mixed(MixedPolicy<true>{});
+        else mixed(MixedPolicy<false>{});
+    } else {
+        if (m.overlap) fp64(Fp64Policy<true>{});
+        else fp64(Fp64Policy<false>{});
     }
     return cudaGetLastError();
 }
