@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmagritte_b200.so")
+LIB_PATH = os.environ.get("MAGRITTE_B200_LIB") or os.path.join(HERE, "libmagritte_b200.so")
 
 MGR_OK = 0
 STATUS_NAMES = {
@@ -79,7 +79,7 @@ def load(build_if_missing: bool = True):
     global _lib
     if _lib is not None:
         return _lib
-    if build_if_missing:
+    if build_if_missing and LIB_PATH == os.path.join(HERE, "libmagritte_b200.so"):
         from . import build as _build
         if _build.stale():
             _build.build()
