@@ -31,7 +31,8 @@ typedef enum {
     MGR_ERR_TIMEOUT = 6,       /* a bounded device wait ran out              */
     MGR_ERR_UNSUPPORTED = 7,   /* input outside what the device path covers  */
     MGR_ERR_STATE = 8,         /* called before the step it depends on       */
-    MGR_ERR_NO_MEMORY = 9      /* a device allocation failed                 */
+    MGR_ERR_NO_MEMORY = 9,     /* a device allocation failed                 */
+    MGR_ERR_TOO_LARGE = 10     /* input larger than a fixed capacity         */
 } mgr_status;
 
 typedef enum {
@@ -236,6 +237,34 @@ mgr_status mgr_timer_stop(mgr_handle *h, double *ms);
 /* Number of this library's kernels launched on the handle since it was
  * created (library kernels such as CUB's prefix sum are not counted). */
 mgr_status mgr_get_launch_count(mgr_handle *h, int64_t *count);
+
+/* --- without allocation ------------------------------------------------- */
+
+/* Largest ncells * nlev that mgr_convergence_noalloc accepts. */
+#define MGR_NOALLOC_MAX_ELEMENTS 67108864LL
+
+/* Convergence statistics of populations `pop` against `prev`, for callers
+ * that cannot allocate device memory: applications that reserve all of the
+ * GPU's memory up front in their own pool and do not allow cudaMalloc (which
+ * would also synchronise the device).  No counterpart in the reference; it
+ * computes what check_for_convergence does, with no handle.
+ *   pop, prev  [ncells*nlev] device arrays, cell-major
+ *   pop_tot    [ncells] device array (total population per cell)
+ *   stats      device array of 3 doubles, receives the fraction of levels
+ *              (with n > 1e-10 n_tot) whose 2|n-n'|/(n+n') exceeds
+ *              pop_prec, the mean of that change over ncells*nlev, its max
+ *   stream     cudaStream_t to run on (NULL: the default stream)
+ * Calls no allocator.  Its scratch is a fixed 1.5 MiB array inside the
+ * library that every GPU loading the library holds until the process exits;
+ * ncells*nlev above MGR_NOALLOC_MAX_ELEMENTS returns MGR_ERR_TOO_LARGE.  The
+ * first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (on different streams) race; nothing in it needs
+ * clearing between calls.  Asynchronous: results are in `stats` once the
+ * stream reaches that point. */
+mgr_status mgr_convergence_noalloc(const double *pop, const double *prev, const double *pop_tot,
+                                   int64_t ncells, int32_t nlev, double pop_prec, double *stats,
+                                   void *stream);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@ STATUS_NAMES = {
     0: "MGR_OK", 1: "MGR_ERR_INVALID_ARG", 2: "MGR_ERR_TRACE", 3: "MGR_ERR_LU_SINGULAR",
     4: "MGR_ERR_NOT_CONVERGED", 5: "MGR_ERR_CUDA", 6: "MGR_ERR_TIMEOUT",
     7: "MGR_ERR_UNSUPPORTED", 8: "MGR_ERR_STATE", 9: "MGR_ERR_NO_MEMORY",
+    10: "MGR_ERR_TOO_LARGE",
 }
 MGR_FP64 = 0
 MGR_MIXED = 1
@@ -34,7 +35,9 @@ EXPORTS = (
     "mgr_get_populations", "mgr_get_J", "mgr_get_Jlin", "mgr_get_Jeff", "mgr_get_lambda",
     "mgr_get_emissivity_opacity", "mgr_get_frequencies", "mgr_get_solve_stats",
     "mgr_synchronize", "mgr_timer_start", "mgr_timer_stop", "mgr_get_launch_count",
+    "mgr_convergence_noalloc",
 )
+NOALLOC_MAX_ELEMENTS = 67108864
 
 _P = C.c_void_p
 _i64 = C.c_int64
@@ -114,6 +117,7 @@ def load(build_if_missing: bool = True):
         getattr(L, n).argtypes = [_P, _P]
     L.mgr_get_emissivity_opacity.argtypes = [_P, _P, _P]
     L.mgr_get_solve_stats.argtypes = [_P, C.POINTER(_dbl), C.POINTER(_dbl)]
+    L.mgr_convergence_noalloc.argtypes = [_P, _P, _P, _i64, _i32, _dbl, _P, _P]
     _lib = L
     return L
 
