@@ -238,6 +238,67 @@ mgr_status mgr_timer_stop(mgr_handle *h, double *ms);
  * created (library kernels such as CUB's prefix sum are not counted). */
 mgr_status mgr_get_launch_count(mgr_handle *h, int64_t *count);
 
+/* --- learned warm start ------------------------------------------------- */
+
+/* Per-cell features and hidden width of the warm-start network. */
+#define MGR_MLP_FEATURES 10
+#define MGR_MLP_HIDDEN 128
+
+/* A 3 x 128 tanh MLP mapping standardised features to a correction of the
+ * LTE log level fractions: n = n_tot softmax(log x_LTE + MLP(f)).
+ * params holds W0 [128 x nin], b0, W1 [128 x 128], b1, W2, b2,
+ * W3 [nout x 128], b3 (row-major, out x in). */
+typedef struct {
+    int32_t nin;           /* MGR_MLP_FEATURES                            */
+    int32_t nout;          /* number of levels                            */
+    float *params;         /* [mgr_mlp_param_count]                       */
+    const float *feat_mean;   /* [nin] feature standardisation            */
+    const float *feat_istd;   /* [nin]                                    */
+} mgr_mlp;
+
+typedef struct {
+    int32_t epochs;
+    int32_t batch;
+    float lr;
+    float weight_decay;
+    uint64_t seed;         /* shuffling                                   */
+} mgr_train_opts;
+
+/* Number of floats in params for a network with nout levels. */
+mgr_status mgr_mlp_param_count(int32_t nout, int64_t *count);
+
+/* Features [ncells*MGR_MLP_FEATURES] of the uploaded model: log10 of the
+ * collision-partner density, n_tot, T, line width, velocity-gradient
+ * length, mean/min column density and mean/min velocity-coherent column
+ * along the traced rays, mean ray length.  No counterpart in the reference. */
+mgr_status mgr_get_features(mgr_handle *h, float *features);
+
+/* LTE log fractions [ncells*nlev] of the uploaded model. */
+mgr_status mgr_get_lte_logfrac(mgr_handle *h, float *logfrac);
+
+/* Warm start: features, network and populations on the device, then
+ * emissivities and opacities; replaces the LTE start
+ * (Simulation::compute_LTE_level_populations, Simulation/sim_lines.tpp:10-16)
+ * before mgr_compute_level_populations.  No counterpart in the reference. */
+mgr_status mgr_warm_start(mgr_handle *h, const mgr_mlp *net);
+
+/* Trains net->params in place on device `device` with this library's own
+ * forward, backward and Adam kernels.  X [n*nin] raw features, lte and
+ * target [n*nout] log fractions (target: converged populations).
+ * loss_hist (optional) receives the mean loss of each epoch. */
+mgr_status mgr_mlp_train(int device, mgr_mlp *net, const float *X, const float *lte,
+                         const float *target, int64_t n, const mgr_train_opts *opts,
+                         float *loss_hist);
+
+/* Network output (the log-fraction correction) [n*nout] for features X. */
+mgr_status mgr_mlp_forward(int device, const mgr_mlp *net, const float *X, int64_t n,
+                           float *delta);
+
+/* Summed loss over n samples and its gradient with respect to params
+ * (for gradient checks). */
+mgr_status mgr_mlp_loss_grad(int device, const mgr_mlp *net, const float *X, const float *lte,
+                             const float *target, int64_t n, float *loss, float *grad);
+
 /* --- without allocation ------------------------------------------------- */
 
 /* Largest ncells * nlev that mgr_convergence_noalloc accepts. */

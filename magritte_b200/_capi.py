@@ -35,8 +35,11 @@ EXPORTS = (
     "mgr_get_populations", "mgr_get_J", "mgr_get_Jlin", "mgr_get_Jeff", "mgr_get_lambda",
     "mgr_get_emissivity_opacity", "mgr_get_frequencies", "mgr_get_solve_stats",
     "mgr_synchronize", "mgr_timer_start", "mgr_timer_stop", "mgr_get_launch_count",
-    "mgr_convergence_noalloc",
+    "mgr_convergence_noalloc", "mgr_mlp_param_count", "mgr_get_features", "mgr_get_lte_logfrac",
+    "mgr_warm_start", "mgr_mlp_train", "mgr_mlp_forward", "mgr_mlp_loss_grad",
 )
+MLP_FEATURES = 10
+MLP_HIDDEN = 128
 NOALLOC_MAX_ELEMENTS = 67108864
 
 _P = C.c_void_p
@@ -61,6 +64,16 @@ class ModelDesc(C.Structure):
                 ("population_tot", _P), ("nquads", _i32), ("ncolpar", _i32),
                 ("quad_roots", _P), ("quad_weights", _P), ("colpar", _P), ("pop_prec", _dbl),
                 ("max_width_fraction", _dbl)]
+
+
+class MlpDesc(C.Structure):
+    _fields_ = [("nin", _i32), ("nout", _i32), ("params", _P), ("feat_mean", _P),
+                ("feat_istd", _P)]
+
+
+class TrainOpts(C.Structure):
+    _fields_ = [("epochs", _i32), ("batch", _i32), ("lr", C.c_float), ("weight_decay", C.c_float),
+                ("seed", C.c_uint64)]
 
 
 class AliOpts(C.Structure):
@@ -118,6 +131,13 @@ def load(build_if_missing: bool = True):
     L.mgr_get_emissivity_opacity.argtypes = [_P, _P, _P]
     L.mgr_get_solve_stats.argtypes = [_P, C.POINTER(_dbl), C.POINTER(_dbl)]
     L.mgr_convergence_noalloc.argtypes = [_P, _P, _P, _i64, _i32, _dbl, _P, _P]
+    L.mgr_mlp_param_count.argtypes = [_i32, C.POINTER(_i64)]
+    L.mgr_get_features.argtypes = [_P, _P]
+    L.mgr_get_lte_logfrac.argtypes = [_P, _P]
+    L.mgr_warm_start.argtypes = [_P, C.POINTER(MlpDesc)]
+    L.mgr_mlp_train.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _P, _P, _i64, C.POINTER(TrainOpts), _P]
+    L.mgr_mlp_forward.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _i64, _P]
+    L.mgr_mlp_loss_grad.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _P, _P, _i64, _P, _P]
     _lib = L
     return L
 

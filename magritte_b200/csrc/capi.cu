@@ -12,6 +12,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <memory>
 #include <stdexcept>
 
 #include "mgr_internal.cuh"
@@ -938,6 +939,85 @@ mgr_status mgr_timer_stop(mgr_handle *h, double *ms) {
         float f = 0.f;
         ck(cudaEventElapsedTime(&f, h->tev0, h->tev1), "elapsed");
         *ms = f;
+    });
+}
+
+// Features of every origin into a device buffer [N*MGR_MLP_FEATURES].
+static void device_features(mgr_handle *h, float *dF) {
+    if (!h->traced) do_trace(h);
+    if (h->stored) {
+        TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
+        ck(launch_features(h->mv, t, dF, h->stream), "features");
+        h->launches += 1;
+    } else {
+        for (int64_t o0 = 0; o0 < h->N; o0 += h->batch_origins) {
+            const int64_t cnt = std::min(h->batch_origins, h->N - o0);
+            TraceView t = build_batch(h, o0, cnt);
+            ck(launch_features(h->mv, t, dF + o0 * MGR_MLP_FEATURES, h->stream), "features");
+            h->launches += 2;
+        }
+    }
+}
+
+mgr_status mgr_get_features(mgr_handle *h, float *features) {
+    return run(h, [&] {
+        need(h->model_loaded && features, MGR_ERR_INVALID_ARG, "no model or NULL output");
+        set_device(h);
+        float *dF = dalloc<float>(h, h->N * MGR_MLP_FEATURES, nullptr);
+        std::unique_ptr<void, decltype(&cudaFree)> guard(dF, &cudaFree);
+        device_features(h, dF);
+        ck(cudaMemcpyAsync(features, dF, h->N * MGR_MLP_FEATURES * sizeof(float),
+                           cudaMemcpyDeviceToHost, h->stream), "d2h");
+        ck(cudaStreamSynchronize(h->stream), "features sync");
+    });
+}
+
+mgr_status mgr_get_lte_logfrac(mgr_handle *h, float *logfrac) {
+    return run(h, [&] {
+        need(h->model_loaded && logfrac, MGR_ERR_INVALID_ARG, "no model or NULL output");
+        set_device(h);
+        float *dL = dalloc<float>(h, h->N * h->nlev, nullptr);
+        std::unique_ptr<void, decltype(&cudaFree)> guard(dL, &cudaFree);
+        ck(launch_lte_logfrac(h->mv, 0, h->N, dL, h->stream), "lte logfrac");
+        h->launches += 1;
+        ck(cudaMemcpyAsync(logfrac, dL, h->N * h->nlev * sizeof(float), cudaMemcpyDeviceToHost,
+                           h->stream), "d2h");
+        ck(cudaStreamSynchronize(h->stream), "sync");
+    });
+}
+
+mgr_status mgr_warm_start(mgr_handle *h, const mgr_mlp *net) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        need(net && net->params && net->feat_mean && net->feat_istd, MGR_ERR_INVALID_ARG, "bad network");
+        need(net->nin == MGR_MLP_FEATURES && net->nout == h->nlev, MGR_ERR_INVALID_ARG,
+             "network shape does not match the model (features, levels)");
+        set_device(h);
+        const int64_t N = h->N, np = mlp_param_count(net->nin, net->nout);
+        std::vector<void *> tmp;
+        struct Free {
+            std::vector<void *> &v;
+            ~Free() { for (void *p : v) cudaFree(p); }
+        } fr{tmp};
+        float *dF = dalloc<float>(h, N * MGR_MLP_FEATURES, &tmp);
+        float *dL = dalloc<float>(h, N * h->nlev, &tmp);
+        float *dD = dalloc<float>(h, N * h->nlev, &tmp);
+        MlpDevice d;
+        d.nin = net->nin;
+        d.nout = net->nout;
+        float *P = upload(h, net->params, np, &tmp);
+        d.mean = upload(h, net->feat_mean, net->nin, &tmp);
+        d.istd = upload(h, net->feat_istd, net->nin, &tmp);
+        mlp_bind(P, d.nin, d.nout, d.W, d.b);
+        ck(mlp_prepare(), "mlp attributes");
+        device_features(h, dF);
+        ck(launch_lte_logfrac(h->mv, 0, N, dL, h->stream), "lte logfrac");
+        ck(launch_mlp_forward(d, dF, N, dD, h->stream), "mlp forward");
+        ck(launch_warm_populations(h->mv, 0, N, dL, dD, h->pop, h->stream), "warm populations");
+        ck(launch_emissivity_opacity(h->mv, level_args(h), h->stream), "emissivity");
+        h->launches += 4;
+        ck(cudaStreamSynchronize(h->stream), "warm start sync");
+        h->pops_valid = true;
     });
 }
 

@@ -158,4 +158,30 @@ cudaError_t launch_convergence(const ModelView &m, const LevelArgs &a, cudaStrea
 cudaError_t launch_ng(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 int level_partials_needed(const ModelView &m);
 
+// Warm-start network on the device (pointers into one parameter buffer).
+struct MlpDevice {
+    int nin, nout;
+    float *W[4], *b[4];
+    float *mean, *istd;
+};
+struct MlpGrad {
+    float *W[4], *b[4];
+};
+size_t mlp_smem_bytes(bool train);
+cudaError_t mlp_prepare();
+cudaError_t launch_mlp_forward(const MlpDevice &d, const float *X, int64_t n, float *out,
+                               cudaStream_t s);
+cudaError_t launch_mlp_train_batch(const MlpDevice &d, const MlpGrad &g, const float *X,
+                                   const float *lte, const float *tgt, const int *idx, int64_t b0,
+                                   int64_t bn, float scale, float *loss, cudaStream_t s);
+cudaError_t launch_adam(float *p, const float *g, float *m, float *v, int64_t n, float lr,
+                        float b1, float b2, int step, float eps, float wd, cudaStream_t s);
+cudaError_t launch_features(const ModelView &m, const TraceView &t, float *F, cudaStream_t s);
+cudaError_t launch_lte_logfrac(const ModelView &m, int64_t o0, int64_t cnt, float *L, cudaStream_t s);
+cudaError_t launch_warm_populations(const ModelView &m, int64_t o0, int64_t cnt, const float *L,
+                                    const float *D, double *pop, cudaStream_t s);
+// parameter layout: W0,b0,W1,b1,W2,b2,W3,b3
+int64_t mlp_param_count(int nin, int nout);
+void mlp_bind(float *base, int nin, int nout, float **W, float **b);
+
 }  // namespace mgr

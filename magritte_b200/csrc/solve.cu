@@ -49,7 +49,7 @@ constexpr int kWarpsPerBlock = 4;
 #endif
 constexpr int kMinBlocks = MGR_SOLVE_MIN_BLOCKS;   // 7: 28 warps per SM (measured best of 4..8)
 
-// 1/x for positive normal x: hardware estimate refined by two Newton-Raphson
+// 1/x for normal x of either sign: hardware estimate refined by two Newton-Raphson
 // steps y <- y (2 - x y) (accurate to about one ulp).
 __device__ __forceinline__ double rcp_pos(double x) {
     double y;
@@ -120,9 +120,35 @@ __device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
 
 // ---------------------------------------------------------------- policies
 
+// Emissivity and opacity at (cell p, frequency freq) over lines [lo, hi]:
+// Simulation::get_eta_and_chi (simulation.tpp:385-481) over the lines in the
+// bin's window, with Thermodynamics::profile (thermodynamics.tpp:16-29);
+// 1/exp(x^2) is written exp(-x^2) and 1/width (1/line)(1/pw).
+__device__ __forceinline__ void eta_chi_double(const ModelView &m, const double *__restrict__ eps,
+                                               const double *__restrict__ kap, int p, double freq,
+                                               int lo, int hi, double &eta, double &chi) {
+    eta = 0.0;
+    chi = 1.0E-26;
+    const double pwp = __ldg(m.pw + p);
+    const double ipw = __ldg(m.inv_pw + p);
+    const int K = m.nrad;
+    for (int l = lo; l <= hi; l++) {
+        const double line_l = __ldg(m.line + l);
+        const double width = line_l * pwp;
+        const double diff = freq - line_l;
+        const bool in = diff <= 11.0 * width && diff >= -11.0 * width;
+        const double inv_w = __ldg(m.inv_line + l) * ipw;
+        const double x = inv_w * diff;
+        const double fp = in ? freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x))) : 0.0;
+        eta += __ldg(eps + (unsigned)p * K + l) * fp;
+        chi += __ldg(kap + (unsigned)p * K + l) * fp;
+    }
+}
+
 template <bool kOverlap>
 struct Fp64Policy {
     using Real = double;
+    static constexpr bool kFallback = false;
     struct Pt {
         int cell;
         double shift, dz;
@@ -141,29 +167,11 @@ struct Fp64Policy {
     __device__ __forceinline__ double freq(const Pt &p, const BinCtx &b) const {
         return p.shift * b.nu_o;
     }
-    // Simulation::get_eta_and_chi (simulation.tpp:385-481) over the lines in
-    // the bin's window, with Thermodynamics::profile (thermodynamics.tpp:16-29);
-    // 1/exp(x^2) is written exp(-x^2) and 1/width (1/line)(1/pw).  Without
-    // overlapping profiles the window holds the bin's own line only.
+    // Without overlapping profiles the window holds the bin's own line only.
     __device__ __forceinline__ void eval(const ModelView &m, int p, double freq, const BinCtx &b,
                                          double &chi, double &t) const {
-        double eta = 0.0;
-        chi = 1.0E-26;
-        const double pwp = __ldg(m.pw + p);
-        const double ipw = __ldg(m.inv_pw + p);
-        const int K = m.nrad;
-        const int lo = kOverlap ? b.lo : b.k, hi = kOverlap ? b.hi : b.k;
-        for (int l = lo; l <= hi; l++) {
-            const double line_l = __ldg(m.line + l);
-            const double width = line_l * pwp;
-            const double diff = freq - line_l;
-            const bool in = diff <= 11.0 * width && diff >= -11.0 * width;
-            const double inv_w = __ldg(m.inv_line + l) * ipw;
-            const double x = inv_w * diff;
-            const double fp = in ? freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x))) : 0.0;
-            eta += __ldg(eps + (unsigned)p * K + l) * fp;
-            chi += __ldg(kap + (unsigned)p * K + l) * fp;
-        }
+        double eta;
+        eta_chi_double(m, eps, kap, p, freq, kOverlap ? b.lo : b.k, kOverlap ? b.hi : b.k, eta, chi);
         t = eta * rcp_pos(chi);
     }
     __device__ __forceinline__ void eval_pt(const ModelView &m, const Pt &p, const BinCtx &b,
@@ -174,16 +182,18 @@ struct Fp64Policy {
         return 0.5 * (chi_a + chi_b) * dz;
     }
     __device__ __forceinline__ static double dz_of(const Pt &p) { return p.dz; }
+    // origin: opacity, source function and the opacity in physical units
     __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
-                                           double &chi, double &t) const {
+                                           double &chi, double &t, double &chi_phys) const {
         eval(m, o, b.nu_o, b, chi, t);
+        chi_phys = chi;
     }
-    __device__ __forceinline__ double to_phys(double chi) const { return chi; }
 };
 
 template <bool kOverlap>
 struct MixedPolicy {
     using Real = float;
+    static constexpr bool kFallback = true;   // redo non-finite pairs in double
     using Pt = MixedPoint;
     const MixedPoint *mp;
     const float2 *ek;         // [N*K] (eps, kap) * INVSQRTPI / pw * X
@@ -239,22 +249,33 @@ struct MixedPolicy {
             eta += (float)(ea * m.mixed_scale);
             chi += (float)(ca * m.mixed_scale);
         }
+        if (chi < floor_hat) {
+            // Negative line opacity (population inversion, which the
+            // reference's iteration allows): float cancels badly near zero,
+            // so this point is evaluated in double as in the FP64 path.
+            double e64, c64;
+            eta_chi_double(m, eps, kap, p.cell, freq(p, b), kOverlap ? b.lo : b.k,
+                           kOverlap ? b.hi : b.k, e64, c64);
+            chi = (float)(c64 * m.mixed_scale);
+            t = (float)(e64 / c64);
+            return;
+        }
         t = __fdividef(eta, chi);
     }
     __device__ __forceinline__ static double dtau(float chi_a, float chi_b, float dzs) {
         return (double)((chi_a + chi_b) * dzs);
     }
     __device__ __forceinline__ static float dz_of(const Pt &p) { return p.dzs; }
+    // origin: evaluated in double once per chunk (it enters every pair and
+    // the ALO), then scaled to the float units of the chains
     __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
-                                           float &chi, float &t) const {
-        Pt p;
-        p.cell = o;
-        p.delta = 0.0f;
-        p.dzs = 0.0f;
-        p.ipw = (float)__ldg(m.inv_pw + o);
-        eval_pt(m, p, b, chi, t);
+                                           float &chi, float &t, double &chi_phys) const {
+        double e64, c64;
+        eta_chi_double(m, eps, kap, o, b.nu_o, kOverlap ? b.lo : b.k, kOverlap ? b.hi : b.k, e64, c64);
+        chi = (float)(c64 * m.mixed_scale);
+        t = (float)(e64 / c64);
+        chi_phys = c64;
     }
-    __device__ __forceinline__ double to_phys(float chi) const { return (double)chi * inv_scale; }
 };
 
 // ------------------------------------------------------------------ chains
@@ -376,6 +397,24 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
     L = iAC * den;
 }
 
+// One ray pair of one bin in double, for the rare lanes where the mixed
+// sweep produced a non-finite result (near-zero or negative opacities from
+// transient population inversion, where float runs out of range).
+__device__ __noinline__ void fp64_pair(const ModelView &m, const TraceView &t, const double *eps,
+                                       const double *kap, const BinCtx &b, int64_t ofr, int nfr,
+                                       int64_t obk, int nbk, int o, DevFlags *flags, double &u,
+                                       double &L) {
+    Fp64Policy<true> pol;
+    pol.cell = t.cell;
+    pol.shift = t.shift;
+    pol.dZ = t.dZ;
+    pol.eps = eps;
+    pol.kap = kap;
+    double chi_o, t_o, chi_phys;
+    pol.origin(m, o, b, chi_o, t_o, chi_phys);
+    sweep<Fp64Policy<true>>(m, pol, b, ofr, nfr, obk, nbk, chi_o, t_o, o, flags, u, L);
+}
+
 template <class Pol>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     formal_solve_kernel(ModelView m, TraceView t, SolveArgs a, Pol pol, DevFlags *flags) {
@@ -409,13 +448,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
 
         // origin: same opacity and source for every pair
         Real chi_o, t_o;
-        pol.origin(m, o, b, chi_o, t_o);
+        double chi_o_d;
+        pol.origin(m, o, b, chi_o, t_o, chi_o_d);
         // ALO factor without the pair weight (raypair_lambda.tpp:26-29, :115-121)
         const double width_o = line_k * pw_o;
         const double iw = 1.0 / width_o;
         const double xo = iw * (b.nu_o - line_k);
         const double prof_o = iw * kINVERSE_SQRT_PI * exp(-(xo * xo));
-        const double chi_o_d = pol.to_phys(chi_o);
         const double lam_pre = m.A[b.k] * (m.qw[z] * 2.0) * (b.nu_o * prof_o / chi_o_d);
 
         double Jf = 0.0, Lf = 0.0;
@@ -442,6 +481,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
             }
             double u, L;
             sweep<Pol>(m, pol, b, ofr, nfr, obk, nbk, chi_o, t_o, o, flags, u, L);
+            if (Pol::kFallback && !(isfinite(u) && isfinite(L)))
+                fp64_pair(m, t, pol.eps, pol.kap, b, ofr, nfr, obk, nbk, o, flags, u, L);
             Jf += 2.0 * wr * u;
             Lf += lam_pre * wr * L;
         }

@@ -284,7 +284,11 @@ def linear_rotor_species(nlev: int, B: float = 57.6e9, mu_debye: float = 0.11,
     """Rigid linear rotor: E_J = h B J (J+1), g = 2J+1, lines J -> J-1 at
     nu = 2 B J with dipole Einstein A; collisional rates from a seeded
     power law Cd(J->J') = C0 (dJ)^-alpha (T/100 K)^beta, Ce by detailed
-    balance."""
+    balance.  C0 (2e-17..6e-17 m^3/s) and alpha (2..2.6) follow the size and
+    the dJ fall-off of CO-H2 rate tables: weaker coupling or a flatter
+    fall-off lets collisional pumping and the radiative cascade invert the
+    lowest levels at the wind's densities, and the reference's local-ALO
+    iteration does not settle in such masing cells."""
     rng = np.random.default_rng(seed)
     J = np.arange(nlev, dtype=np.float64)
     energy = HH * B * J * (J + 1.0)
@@ -298,8 +302,8 @@ def linear_rotor_species(nlev: int, B: float = 57.6e9, mu_debye: float = 0.11,
     if tmp is None:
         tmp = np.array([10.0, 20.0, 50.0, 100.0, 200.0, 500.0, 1000.0, 2000.0, 3000.0])
     tmp = np.asarray(tmp, dtype=np.float64)
-    C0 = 10 ** rng.uniform(-17.3, -16.7)
-    alpha = rng.uniform(0.8, 1.4)
+    C0 = 10 ** rng.uniform(-16.7, -16.2)
+    alpha = rng.uniform(2.0, 2.6)
     beta = rng.uniform(0.1, 0.4)
     ic, jc = [], []
     for i in range(1, nlev):

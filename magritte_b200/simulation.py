@@ -219,6 +219,22 @@ class Simulation:
         self._ck(self._lib.mgr_get_launch_count(self._h, C.byref(n)))
         return n.value
 
+    # ------------------------------------------------------ learned start
+    def features(self) -> np.ndarray:
+        out = np.zeros((self.model.ncells, _capi.MLP_FEATURES), np.float32)
+        self._ck(self._lib.mgr_get_features(self._h, out.ctypes.data))
+        return out
+
+    def lte_logfrac(self) -> np.ndarray:
+        out = np.zeros((self.model.ncells, self.model.linedata.nlev), np.float32)
+        self._ck(self._lib.mgr_get_lte_logfrac(self._h, out.ctypes.data))
+        return out
+
+    def warm_start(self, net) -> int:
+        """Learned start (replaces compute_LTE_level_populations)."""
+        d = net.desc()
+        return self._ck(self._lib.mgr_warm_start(self._h, C.byref(d)))
+
     def solve_stats(self):
         ms, up = C.c_double(), C.c_double()
         self._ck(self._lib.mgr_get_solve_stats(self._h, C.byref(ms), C.byref(up)))
