@@ -3,10 +3,12 @@
 Workload (default): the 64^3 jittered spherical wind (262,144 cells, 10-level
 linear rotor, 9 lines x 31 bins = 279 bins, 48 HEALPix rays = 24 pairs),
 seeded synthetic data.  One step is one complete solve of the hot path:
-trace every ray, start from LTE populations, and iterate formal solve +
-Jeff + statistical equilibrium (+ Ng every 5th iteration) until the max
-relative population change over all (cell, level) with n > 1e-10 n_tot
-drops below 1e-4.
+trace every ray, set the starting populations (learned warm start by
+default, LTE with --start lte), and iterate formal solve + Jeff +
+statistical equilibrium (+ Ng every 5th iteration) until the max relative
+population change over all (cell, level) with n > 1e-10 n_tot drops below
+1e-4.  The headline arm is learned start + mixed precision; the plain FP64
+solve from LTE is measured in the same run and reported beside it.
 
     value  seconds per converged solve, device-timed (CUDA events on the
            library's stream), model already resident in HBM
@@ -49,10 +51,14 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--start", default="learned", choices=["learned", "lte"])
+    ap.add_argument("--weights", default=os.path.join(ROOT, "magritte_b200", "weights",
+                                                      "wind_rotor10.npz"))
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
     ap.add_argument("--workload", default="wind64", choices=["wind64", "lattice16"])
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -66,12 +72,12 @@ def make_model(name):
     return M.config1()
 
 
-def workload_config(name, model, prec):
+def workload_config(name, model, prec, start="LTE"):
     return {"workload": "64^3 spherical wind, 10-level rotor" if name == "wind64"
             else "16^3 lattice cloud, 2-level line",
             "cells": model.ncells, "levels": model.linedata.nlev, "lines": model.nlines,
             "bins_per_line": model.nquads, "rays": model.nrays,
-            "start": "LTE", "tol_max_rel": TOL, "ng": True, "precision": prec,
+            "start": start, "tol_max_rel": TOL, "ng": True, "precision": prec,
             "l2": "inputs larger than L2 (ray traces of several GB re-read every iteration)"}
 
 
@@ -143,41 +149,51 @@ def peaks():
 
 # ------------------------------------------------------------------ CPU arm
 
-def cpu_oracle_time(model, iterations, sample_s, nthreads=None):
-    """The CPU oracle on this host: a formal solve over a seeded sample of
-    origins (all ray pairs), scaled to all origins, plus one full
-    rate-equation step, times the iteration count."""
-    import numpy as np
-    import oracle
-    nthreads = nthreads or os.cpu_count() or 1
-    o = oracle.Oracle(model).setup()
-    rng = np.random.default_rng(0)
-    n = 64
-    t_solve = None
-    while True:
-        origins = np.sort(rng.choice(model.ncells, size=min(n, model.ncells), replace=False))
+class CpuOracle:
+    """The CPU oracle on this host's cores (OpenMP over origins, as the
+    reference): one formal solve over a seeded sample of origins (all ray
+    pairs) scaled to all origins, plus one full rate-equation step, times
+    the iteration count of the solve."""
+
+    def __init__(self, model, nthreads=None):
+        import oracle
+        self.model = model
+        self.nthreads = nthreads or os.cpu_count() or 1
+        self.o = oracle.Oracle(model).setup()
+
+    def time(self, iterations, sample_s, seed=0):
+        import numpy as np
+        m, o = self.model, self.o
+        rng = np.random.default_rng(seed)
+        n = 64
+        while True:
+            origins = np.sort(rng.choice(m.ncells, size=min(n, m.ncells), replace=False))
+            t0 = time.perf_counter()
+            o.compute_radiation_field(origins=origins, nthreads=self.nthreads)
+            dt = time.perf_counter() - t0
+            if dt > 0.25 * sample_s or n >= m.ncells:
+                t_solve = dt * m.ncells / len(origins)
+                break
+            n = min(m.ncells, int(n * max(2.0, 0.3 * sample_s / max(dt, 1e-3))))
         t0 = time.perf_counter()
-        o.compute_radiation_field(origins=origins, nthreads=nthreads)
-        dt = time.perf_counter() - t0
-        if dt > 0.25 * sample_s or n >= model.ncells:
-            t_solve = dt * model.ncells / len(origins)
-            break
-        n = min(model.ncells, int(n * max(2.0, 0.3 * sample_s / max(dt, 1e-3))))
-    t0 = time.perf_counter()
-    o.compute_Jeff()
-    o.compute_level_populations_from_stateq()
-    t_stateq = time.perf_counter() - t0
-    per_iter = t_solve + t_stateq
-    return {"seconds": per_iter * iterations, "per_iteration_s": per_iter,
-            "formal_solve_s": t_solve, "stateq_s": t_stateq, "sample_origins": int(len(origins)),
-            "cores": nthreads}
+        o.compute_Jeff()
+        o.compute_level_populations_from_stateq()
+        t_stateq = time.perf_counter() - t0
+        per_iter = t_solve + t_stateq
+        return {"seconds": per_iter * iterations, "per_iteration_s": per_iter,
+                "formal_solve_s": t_solve, "stateq_s": t_stateq,
+                "sample_origins": int(len(origins)), "cores": self.nthreads}
+
+
+def cpu_oracle_time(model, iterations, sample_s, nthreads=None):
+    return CpuOracle(model, nthreads).time(iterations, sample_s)
 
 
 # iterations of the FP64 solve of the default workload; the reference arm,
 # which cannot afford the full solve on CPU, multiplies its per-iteration
 # time by the count the same algorithm needs (equal iteration counts of
 # the oracle and the device path are checked by the GPU tests).
-REFERENCE_ITERATIONS = {"wind64": None, "lattice16": None}
+REFERENCE_ITERATIONS = {"wind64": 5, "lattice16": None}
 
 
 def run_reference(args):
@@ -192,13 +208,14 @@ def run_reference(args):
         if o is not None:
             iters, _ = o.compute_level_populations(True, MAX_ITER, TOL)
         else:
-            iters = int(os.environ.get("MGR_REFERENCE_ITERATIONS", "0")) or 30
+            iters = 5
+    cpu = CpuOracle(model)
+    for w in range(args.warmup):
+        cpu.time(iters, min(2.0, args.cpu_sample_s), seed=100 + w)
     steps = []
     info = None
-    for _ in range(args.warmup):
-        pass
-    for _ in range(max(1, args.steps)):
-        info = cpu_oracle_time(model, iters, args.cpu_sample_s)
+    for k in range(max(1, args.steps)):
+        info = cpu.time(iters, args.cpu_sample_s, seed=k)
         steps.append(info["seconds"])
     value = statistics.mean(steps)
     line = {
@@ -232,11 +249,21 @@ def run_b200(args):
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     model = make_model(args.workload)
     prec = args.precision
+    net = None
+    if args.start == "learned":
+        from magritte_b200.learned import WarmStartNet
+        net = WarmStartNet.load(args.weights)
 
-    def one_solve(sim):
+    def start(sim, learned):
+        if learned:
+            sim.warm_start(net)
+        else:
+            sim.compute_LTE_level_populations()
+
+    def one_solve(sim, learned=net is not None, precision=prec):
         sim.trace()
-        sim.compute_LTE_level_populations()
-        return sim.compute_level_populations(True, MAX_ITER, prec, tol_max_rel=TOL)
+        start(sim, learned)
+        return sim.compute_level_populations(True, MAX_ITER, precision, tol_max_rel=TOL)
 
     # ---- device-resident solve
     sim = Simulation(model, device=local if dist else 0)
@@ -264,19 +291,29 @@ def run_b200(args):
 
     # ---- end to end through the C ABI from host buffers
     e2e = []
-    h2d = model.nbytes() + sum(int(a.nbytes) for a in (model.linedata.energy,))
+    h2d = model.nbytes() + (int(net.params.nbytes) if net is not None else 0)
     d2h = model.ncells * model.linedata.nlev * 8
     for _ in range(max(1, args.steps)):
         t0 = time.perf_counter()
         s2 = Simulation(model, device=local if dist else 0)
         s2.compute_spectral_discretisation()
         s2.compute_boundary_intensities()
-        s2.compute_LTE_level_populations()
+        start(s2, net is not None)
         s2.compute_level_populations(True, MAX_ITER, prec, tol_max_rel=TOL)
         pop = s2.population
         e2e.append(time.perf_counter() - t0)
         s2.close()
     assert np.all(np.isfinite(pop))
+
+    # ---- the plain method: FP64 from the LTE start (north-star comparison)
+    plain = None
+    if not args.no_plain:
+        sim.timer_start()
+        it_p = one_solve(sim, learned=False, precision="fp64")
+        t_p = sim.timer_stop() / 1e3
+        plain = {"start": "LTE", "precision": "fp64", "ali_iterations": it_p, "seconds": t_p,
+                 "converged": bool(getattr(sim, "converged", False))}
+    sim.close()
 
     # ---- multi-GPU: max over ranks
     if dist:
@@ -300,8 +337,9 @@ def run_b200(args):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == "fp64" else "f32+f64",
         "data": "synthetic (seeded)",
-        "config": workload_config(args.workload, model, prec),
+        "config": workload_config(args.workload, model, prec, args.start),
         "ali_iterations": iters[-1], "converged": converged,
+        "plain_fp64_lte": plain,
         "final_max_rel_change": err_hist[-1] if err_hist else None,
         "formal_solve": {"ms": avg_ms, "updates": solve_upd[-1],
                          "updates_per_s": solve_upd[-1] / (avg_ms / 1e3)},

@@ -83,6 +83,7 @@ struct mgr_handle {
     int64_t batch_origins = 0;
     int64_t trace_budget = 0;
     double updates_per_solve = 0.0;
+    int max_pair_points = 0;
     std::vector<int32_t> h_len;        // [nrays*N] host copy for npoints
 
     bool model_loaded = false, line_set = false, bdy_set = false, pops_valid = false;
@@ -90,6 +91,13 @@ struct mgr_handle {
     double last_solve_ms = 0.0, last_updates = 0.0;
 
     std::vector<int64_t> antipod;
+    int64_t nboundary = 0;
+    int64_t *b2c_dev = nullptr;        // boundary -> cell (int64)
+    double *ibdy = nullptr;            // [nboundary][nfreqs]
+    int4 *patch = nullptr;             // mixed solve: entries redone in double
+    unsigned long long *patch_count = nullptr;
+    int64_t patch_cap = 0;
+    int64_t last_patched = 0;
 };
 
 namespace {
@@ -139,7 +147,8 @@ void free_model(mgr_handle *h) {
     void **state[] = {(void **)&h->pop, (void **)&h->prev1, (void **)&h->prev2, (void **)&h->prev3,
                       (void **)&h->eps, (void **)&h->kap, (void **)&h->Jlin, (void **)&h->Lam,
                       (void **)&h->Jeff, (void **)&h->J, (void **)&h->partials, (void **)&h->stats,
-                      (void **)&h->ek, (void **)&h->flags};
+                      (void **)&h->ek, (void **)&h->flags, (void **)&h->ibdy,
+                      (void **)&h->patch, (void **)&h->patch_count};
     for (void **p : state) free_ptr(*p);
     h->model_loaded = h->line_set = h->bdy_set = h->pops_valid = false;
 }
@@ -349,6 +358,8 @@ void do_upload(mgr_handle *h, const mgr_model_desc *d) {
     m.cell2bdy = upload(h, c2b.data(), N, T);
     m.antipod = upload(h, ap32.data(), d->nrays, T);
     m.bdy_T = upload(h, bT.data(), d->nboundary, T);
+    h->nboundary = d->nboundary;
+    h->b2c_dev = upload(h, d->boundary2cell, d->nboundary, T);
     m.T = upload(h, d->temperature, N, T);
     m.dshift_max = upload(h, dsm.data(), N, T);
     m.pw = upload(h, pw.data(), N, T);
@@ -475,6 +486,7 @@ void do_trace(mgr_handle *h) {
     set_device(h);
     free_traces(h);
     const int64_t N = h->N, R = h->nrays, n = R * N;
+    h->max_pair_points = 0;
     if (!h->len_all) h->len_all = dalloc<int32_t>(h, n, nullptr);
     reset_flags(h);
     ck(launch_trace_count(h->mv, 0, N, h->len_all, h->flags, h->stream), "trace count");
@@ -496,6 +508,7 @@ void do_trace(mgr_handle *h) {
         for (int64_t o = 0; o < N; o++) {
             const int64_t ndep = (int64_t)h->h_len[r * N + o] + h->h_len[ar * N + o] + 1;
             if (ndep > 1) U += (double)ndep;
+            h->max_pair_points = std::max<int>(h->max_pair_points, (int)(ndep - 1));
         }
     }
     h->updates_per_solve = U * h->nfreqs;
@@ -555,13 +568,30 @@ TraceView build_batch(mgr_handle *h, int64_t o0, int64_t cnt) {
     return t;
 }
 
+void boundary_table(mgr_handle *h) {
+    if (!h->ibdy) {
+        h->ibdy = dalloc<double>(h, h->nboundary * (int64_t)h->nfreqs, nullptr);
+        h->mv.ibdy = h->ibdy;
+    }
+    ck(launch_boundary_table(h->mv, h->nboundary, h->b2c_dev, h->ibdy, h->stream), "boundary table");
+    h->launches += 1;
+    ck(cudaStreamSynchronize(h->stream), "boundary sync");
+    h->bdy_set = true;
+}
+
 void do_solve(mgr_handle *h, int precision) {
     need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
     need(h->pops_valid, MGR_ERR_STATE, "no level populations yet (LTE or set_populations)");
     need(precision == MGR_FP64 || precision == MGR_MIXED, MGR_ERR_INVALID_ARG, "bad precision");
     set_device(h);
     if (!h->traced) do_trace(h);
+    if (!h->bdy_set) boundary_table(h);
     if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
+    if (precision == MGR_MIXED && !h->patch) {
+        h->patch_cap = 1 << 20;
+        h->patch = dalloc<int4>(h, h->patch_cap, nullptr);
+        h->patch_count = dalloc<unsigned long long>(h, 1, nullptr);
+    }
     SolveArgs a{};
     a.eps = h->eps;
     a.kap = h->kap;
@@ -570,26 +600,49 @@ void do_solve(mgr_handle *h, int precision) {
     a.Jlin = h->Jlin;
     a.Lam = h->Lam;
     a.J = h->keep_J ? h->J : nullptr;
+    a.patch = h->patch;
+    a.patch_count = h->patch_count;
+    a.patch_cap = h->patch_cap;
+    a.max_pair_points = h->max_pair_points;
     reset_flags(h);
+    unsigned long long patched = 0;
+    auto launch = [&](const TraceView &t) {
+        if (precision == MGR_MIXED)
+            ck(cudaMemsetAsync(h->patch_count, 0, sizeof(unsigned long long), h->stream), "patch reset");
+        ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
+        h->launches += precision == MGR_MIXED ? 2 : 1;
+        if (precision == MGR_MIXED) {
+            unsigned long long c = 0;
+            ck(cudaMemcpyAsync(&c, h->patch_count, sizeof(c), cudaMemcpyDeviceToHost, h->stream), "d2h");
+            ck(cudaStreamSynchronize(h->stream), "patch count");
+            patched += c;
+        }
+    };
     ck(cudaEventRecord(h->ev0, h->stream), "event");
     if (h->stored) {
         TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
-        ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
-        h->launches += 1;
+        launch(t);
     } else {
         for (int64_t o0 = 0; o0 < h->N; o0 += h->batch_origins) {
             const int64_t cnt = std::min(h->batch_origins, h->N - o0);
             TraceView t = build_batch(h, o0, cnt);
-            ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
-            h->launches += 1;
+            launch(t);
         }
     }
     ck(cudaEventRecord(h->ev1, h->stream), "event");
+    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream), "flags");
+    ck(cudaStreamSynchronize(h->stream), "solve sync");
+    if (precision == MGR_MIXED && h->h_flags->patch_overflow) {
+        // more float failures than the patch list holds: solve in double
+        do_solve(h, MGR_FP64);
+        return;
+    }
     check_flags(h, "formal solve");
     float ms = 0.f;
     ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
     h->last_solve_ms = ms;
     h->last_updates = h->updates_per_solve;
+    h->last_patched = (int64_t)patched;
 }
 
 void read_stats(mgr_handle *h) {
@@ -726,7 +779,8 @@ mgr_status mgr_compute_spectral_discretisation(mgr_handle *h) {
 mgr_status mgr_compute_boundary_intensities(mgr_handle *h) {
     return run(h, [&] {
         need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
-        h->bdy_set = true;   // evaluated on the fly from the boundary temperatures
+        set_device(h);
+        boundary_table(h);
     });
 }
 

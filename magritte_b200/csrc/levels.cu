@@ -369,6 +369,20 @@ __global__ void ng_update_kernel(ModelView m, LevelArgs a) {
     a.prev1[q] = P;
 }
 
+// Simulation::compute_boundary_intensities (Simulation/sim_radiation.tpp:17-48):
+// I_bdy[b][f] = planck(T_b, nu_p[f]) on the grid of the boundary cell p.
+__global__ void boundary_table_kernel(ModelView m, int64_t nb, const int64_t *b2c, double *table) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * m.nfreqs) return;
+    const int64_t b = idx / m.nfreqs;
+    const int f = (int)(idx - b * m.nfreqs);
+    const int64_t p = b2c[b];
+    const int k = f / m.nquads;
+    const double line = m.line[k];
+    const double nu = radd(line, rmul(rmul(line, m.pw[p]), m.roots[f - k * m.nquads]));
+    table[idx] = planck(m.bdy_T[b], nu);
+}
+
 }  // namespace
 
 int level_partials_needed(const ModelView &m) {
@@ -379,6 +393,13 @@ int level_partials_needed(const ModelView &m) {
 
 static inline unsigned blocks_for(int64_t n, int threads) {
     return (unsigned)((n + threads - 1) / threads);
+}
+
+cudaError_t launch_boundary_table(const ModelView &m, int64_t nboundary, const int64_t *b2c,
+                                  double *table, cudaStream_t s) {
+    boundary_table_kernel<<<blocks_for(nboundary * m.nfreqs, 256), 256, 0, s>>>(m, nboundary, b2c,
+                                                                                 table);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_lte(const ModelView &m, const LevelArgs &a, cudaStream_t s) {

@@ -82,6 +82,7 @@ struct ModelView {
     const int32_t *cell2bdy;
     const int32_t *antipod;
     const double *bdy_T;
+    const double *ibdy;    // [nboundary][nfreqs] boundary intensities
     const double *T, *dshift_max, *pw, *inv_pw;
     const double *line, *inv_line, *A, *Bs, *Ba, *energy, *weight;
     const int32_t *irad, *jrad, *win_lo, *win_hi;
@@ -119,6 +120,7 @@ struct DevFlags {
     unsigned long long lu_err;      // zero pivots
     unsigned long long cap_err;     // trace longer than its slot
     unsigned long long stuck_err;   // step limit reached
+    unsigned long long patch_overflow;  // mixed entries beyond the patch list
 };
 
 // ------------------------------------------------------------------------
@@ -136,6 +138,10 @@ struct SolveArgs {
     double *Jlin, *Lam;             // [N*K]
     double *J;                      // [N*nfreqs] or null
     int warps_per_block;
+    int max_pair_points;            // longest ray pair (both halves) of the trace store
+    int4 *patch;                    // mixed: (origin, pair, bin) to redo in double
+    unsigned long long *patch_count;
+    int64_t patch_cap;
 };
 cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const SolveArgs &a,
                                 int precision, DevFlags *flags, cudaStream_t s);
@@ -151,6 +157,8 @@ struct LevelArgs {
     int npartials;
 };
 cudaError_t launch_lte(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+cudaError_t launch_boundary_table(const ModelView &m, int64_t nboundary, const int64_t *b2c,
+                                  double *table, cudaStream_t s);
 cudaError_t launch_emissivity_opacity(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_jeff(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_stateq(const ModelView &m, const LevelArgs &a, DevFlags *flags, cudaStream_t s);

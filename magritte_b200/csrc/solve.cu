@@ -48,6 +48,14 @@ constexpr int kWarpsPerBlock = 4;
 #define MGR_SOLVE_MIN_BLOCKS 7
 #endif
 constexpr int kMinBlocks = MGR_SOLVE_MIN_BLOCKS;   // 7: 28 warps per SM (measured best of 4..8)
+#ifndef MGR_STAGED_MIN_BLOCKS
+#define MGR_STAGED_MIN_BLOCKS 8
+#endif
+constexpr int kMinBlocksStaged = MGR_STAGED_MIN_BLOCKS;
+#ifndef MGR_STAGED_MAX_POINTS
+#define MGR_STAGED_MAX_POINTS 768
+#endif
+constexpr int kStagedMaxCap = MGR_STAGED_MAX_POINTS;   // points per ray pair in the staged buffer
 
 // 1/x for normal x of either sign: hardware estimate refined by two Newton-Raphson
 // steps y <- y (2 - x y) (accurate to about one ulp).
@@ -65,6 +73,7 @@ struct BinCtx {
     double nu_o;      // bin frequency at the origin (sim_spectrum.tpp:37-41)
     int k;            // line of the bin
     int lo, hi;       // lines whose +-11-width window can reach this bin
+    int f;            // the bin
     float q;          // pw_o * root_z: offset of the bin from its line, in units of nu
 };
 
@@ -72,20 +81,23 @@ struct BinCtx {
 // helper below.
 struct BdyCtx {
     const int32_t *cell2bdy;
-    const double *bdy_T, *pw, *line, *roots;
+    const double *ibdy;            // [nboundary][nfreqs] I_bdy on each boundary cell's grid
+    const double *pw, *line, *roots;
     int nq, nf;
 };
 
 // Radiation::rescale_I_bdy (scalar build, Model/Radiation/radiation.tpp:341-373)
-// with I_bdy = planck(T_b, nu_p) evaluated on the fly.  The grid of cell p is
-// ascending, so the reference's linear notch search equals a lower bound.
-__device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p, DevFlags *flags) {
+// on the table of Simulation::compute_boundary_intensities.  The grid of
+// cell p is ascending, so the reference's linear notch search (first bin with
+// freq <= nu_p) is found by stepping from the lane's own bin f0, which is
+// within a few bins of the answer for Doppler shifts of a few widths.
+__device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p, int f0,
+                                                  DevFlags *flags) {
     const int b = __ldg(c.cell2bdy + p);
     if (b < 0) {
         atomicAdd(&flags->trace_err, 1ull);
         return 0.0;
     }
-    const double T = __ldg(c.bdy_T + b);
     const double pwp = __ldg(c.pw + p);
     const int nq = c.nq, nf = c.nf;
     auto nu_at = [&](int f) {
@@ -93,23 +105,31 @@ __device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p, 
         const double line = __ldg(c.line + k);
         return radd(line, rmul(rmul(line, pwp), __ldg(c.roots + (f - k * nq))));
     };
-    int lo = 0, hi = nf;   // first f with freq <= nu(f), or nf
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (freq <= nu_at(mid)) hi = mid;
-        else lo = mid + 1;
+    int f = f0;
+    int steps = 0;
+    while (f < nf && !(freq <= nu_at(f)) && steps < 16) { f++; steps++; }
+    while (f > 0 && freq <= nu_at(f - 1) && steps < 16) { f--; steps++; }
+    if (steps >= 16) {   // far from the hint: bisect
+        int lo = 0, hi = nf;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (freq <= nu_at(mid)) hi = mid;
+            else lo = mid + 1;
+        }
+        f = lo;
     }
-    const int notch = lo < nf ? lo : nf - 1;
-    if (notch == 0 || notch == nf - 1) return planck(T, nu_at(notch));
+    const int notch = f < nf ? f : nf - 1;
+    const double *I = c.ibdy + (int64_t)b * nf;
+    if (notch == 0 || notch == nf - 1) return __ldg(I + notch);
     const double nu1 = nu_at(notch), nu2 = nu_at(notch - 1);
-    const double I1 = planck(T, nu1), I2 = planck(T, nu2);
+    const double I1 = __ldg(I + notch), I2 = __ldg(I + notch - 1);
     return (I2 - I1) / (nu2 - nu1) * (freq - nu1) + I1;
 }
 
 __device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
     BdyCtx c;
     c.cell2bdy = m.cell2bdy;
-    c.bdy_T = m.bdy_T;
+    c.ibdy = m.ibdy;
     c.pw = m.pw;
     c.line = m.line;
     c.roots = m.roots;
@@ -249,17 +269,11 @@ struct MixedPolicy {
             eta += (float)(ea * m.mixed_scale);
             chi += (float)(ca * m.mixed_scale);
         }
-        if (chi < floor_hat) {
-            // Negative line opacity (population inversion, which the
-            // reference's iteration allows): float cancels badly near zero,
-            // so this point is evaluated in double as in the FP64 path.
-            double e64, c64;
-            eta_chi_double(m, eps, kap, p.cell, freq(p, b), kOverlap ? b.lo : b.k,
-                           kOverlap ? b.hi : b.k, e64, c64);
-            chi = (float)(c64 * m.mixed_scale);
-            t = (float)(e64 / c64);
-            return;
-        }
+        // Negative line opacity (population inversion, which the
+        // reference's iteration allows) cancels badly in float near zero:
+        // such a point poisons its pair with a NaN source function, and the
+        // pair is solved again in double by the patch pass.
+        if (chi < floor_hat) eta = __int_as_float(0x7fc00000);
         t = __fdividef(eta, chi);
     }
     __device__ __forceinline__ static double dtau(float chi_a, float chi_b, float dzs) {
@@ -272,6 +286,66 @@ struct MixedPolicy {
                                            float &chi, float &t, double &chi_phys) const {
         double e64, c64;
         eta_chi_double(m, eps, kap, o, b.nu_o, kOverlap ? b.lo : b.k, kOverlap ? b.hi : b.k, e64, c64);
+        chi = (float)(c64 * m.mixed_scale);
+        t = (float)(e64 / c64);
+        chi_phys = c64;
+    }
+};
+
+// One traced point staged in shared memory for the chunk being solved:
+// the float record plus the scaled opacity pairs of the chunk's two lines.
+struct __align__(16) StagedPt {
+    float delta, dzs, ipw;
+    int cell;
+    float2 e0, e1;
+};
+
+// Mixed precision on points staged in shared memory (no global loads in
+// the sweep).  Indices are positions in the staged buffer.
+struct StagedMixedPolicy {
+    using Real = float;
+    struct Pt {
+        float delta, dzs, ipw;
+        int cell;
+        float2 e;
+    };
+    const StagedPt *pts;
+    bool hi;                  // this lane's bin belongs to the chunk's second line
+    float floor_hat;
+    double inv_scale;
+    const double *eps, *kap;
+
+    __device__ __forceinline__ Pt load(int64_t i) const {
+        const StagedPt &q = pts[i];
+        Pt p;
+        p.delta = q.delta;
+        p.dzs = q.dzs;
+        p.ipw = q.ipw;
+        p.cell = q.cell;
+        p.e = hi ? q.e1 : q.e0;
+        return p;
+    }
+    __device__ __forceinline__ double freq(const Pt &p, const BinCtx &b) const {
+        return (1.0 + (double)p.delta) * b.nu_o;
+    }
+    __device__ __forceinline__ void eval_pt(const ModelView &, const Pt &p, const BinCtx &b,
+                                            float &chi, float &t) const {
+        const float off = fmaf(p.delta, b.q, p.delta + b.q);
+        const float x = off * p.ipw;
+        const float g = fabsf(x) <= 11.0f ? (1.0f + off) * __expf(-x * x) : 0.0f;
+        float eta = p.e.x * g;
+        chi = fmaf(p.e.y, g, floor_hat);
+        if (chi < floor_hat) eta = __int_as_float(0x7fc00000);   // redone in double
+        t = __fdividef(eta, chi);
+    }
+    __device__ __forceinline__ static double dtau(float chi_a, float chi_b, float dzs) {
+        return (double)((chi_a + chi_b) * dzs);
+    }
+    __device__ __forceinline__ static float dz_of(const Pt &p) { return p.dzs; }
+    __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
+                                           float &chi, float &t, double &chi_phys) const {
+        double e64, c64;
+        eta_chi_double(m, eps, kap, o, b.nu_o, b.k, b.k, e64, c64);
         chi = (float)(c64 * m.mixed_scale);
         t = (float)(e64 / c64);
         chi_phys = c64;
@@ -332,7 +406,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
         const auto p = pol.load(ofr + nfr - 1);
         pol.eval_pt(m, p, b, chi, t);
         fr.chi_a = chi; fr.t_a = t; fr.dz_a = Pol::dz_of(p);
-        I0 = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
+        I0 = boundary_intensity(bc, pol.freq(p, b), p.cell, b.f, flags);
     }
     if (nfr >= 2) {
         const auto p = pol.load(ofr + nfr - 2);
@@ -346,7 +420,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
         const auto p = pol.load(obk + nbk - 1);
         pol.eval_pt(m, p, b, chi, t);
         bk.chi_a = chi; bk.t_a = t; bk.dz_a = Pol::dz_of(p);
-        In = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
+        In = boundary_intensity(bc, pol.freq(p, b), p.cell, b.f, flags);
         if (nbk >= 2) {
             const auto q = pol.load(obk + nbk - 2);
             pol.eval_pt(m, q, b, chi, t);
@@ -356,7 +430,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
         }
     } else {
         const int bo = __ldg(m.cell2bdy + origin);
-        if (bo >= 0) In = planck(__ldg(m.bdy_T + bo), b.nu_o);
+        if (bo >= 0) In = __ldg(m.ibdy + (int64_t)bo * m.nfreqs + b.f);
         else atomicAdd(&flags->trace_err, 1ull);
     }
     // both halves have interior points
@@ -397,22 +471,53 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
     L = iAC * den;
 }
 
-// One ray pair of one bin in double, for the rare lanes where the mixed
-// sweep produced a non-finite result (near-zero or negative opacities from
-// transient population inversion, where float runs out of range).
-__device__ __noinline__ void fp64_pair(const ModelView &m, const TraceView &t, const double *eps,
-                                       const double *kap, const BinCtx &b, int64_t ofr, int nfr,
-                                       int64_t obk, int nbk, int o, DevFlags *flags, double &u,
-                                       double &L) {
+// Patch pass of the mixed solve: (origin, pair, bin) entries whose float
+// sweep produced a non-finite u or L (near-zero or negative opacities from
+// transient population inversion, where float runs out of range) are
+// solved again in double, one thread per entry, and added to the outputs.
+__global__ void patch_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = min((unsigned long long)*a.patch_count, (unsigned long long)a.patch_cap);
+    if (i >= n) return;
+    const int4 e = a.patch[i];
+    const int o = e.x, r = e.y, f = e.z;
+    const int64_t oi = o - t.o_begin;
+    const int nq = m.nquads, nf = m.nfreqs, K = m.nrad;
+    BinCtx b;
+    b.f = f;
+    b.k = f / nq;
+    const int z = f - b.k * nq;
+    b.lo = m.win_lo[b.k];
+    b.hi = m.win_hi[b.k];
+    const double line_k = m.line[b.k];
+    const double pw_o = m.pw[o];
+    b.nu_o = radd(line_k, rmul(rmul(line_k, pw_o), m.roots[z]));
+    b.q = (float)(pw_o * m.roots[z]);
+    const int ar = m.antipod[r];
+    const int64_t ir = (int64_t)r * t.o_count + oi, iar = (int64_t)ar * t.o_count + oi;
+    const int nr_ = t.len[ir], nar_ = t.len[iar];
+    const bool rfront = nr_ > nar_;
     Fp64Policy<true> pol;
     pol.cell = t.cell;
     pol.shift = t.shift;
     pol.dZ = t.dZ;
-    pol.eps = eps;
-    pol.kap = kap;
+    pol.eps = a.eps;
+    pol.kap = a.kap;
     double chi_o, t_o, chi_phys;
     pol.origin(m, o, b, chi_o, t_o, chi_phys);
-    sweep<Fp64Policy<true>>(m, pol, b, ofr, nfr, obk, nbk, chi_o, t_o, o, flags, u, L);
+    double u, L;
+    sweep<Fp64Policy<true>>(m, pol, b, rfront ? t.off[ir] : t.off[iar], rfront ? nr_ : nar_,
+                            rfront ? t.off[iar] : t.off[ir], rfront ? nar_ : nr_, chi_o, t_o, o,
+                            flags, u, L);
+    const double wr = m.ray_w[r];
+    const double width_o = line_k * pw_o;
+    const double iw = 1.0 / width_o;
+    const double xo = iw * (b.nu_o - line_k);
+    const double prof_o = iw * kINVERSE_SQRT_PI * exp(-(xo * xo));
+    const double lam_pre = m.A[b.k] * (m.qw[z] * 2.0) * (b.nu_o * prof_o / chi_phys);
+    atomicAdd(a.Jlin + (int64_t)o * K + b.k, m.qw[z] * (2.0 * wr * u));
+    atomicAdd(a.Lam + (int64_t)o * K + b.k, lam_pre * wr * L);
+    if (a.J) atomicAdd(a.J + (int64_t)o * nf + f, 2.0 * wr * u);
 }
 
 template <class Pol>
@@ -437,6 +542,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
         const bool active = f < nf;
         const int fc = active ? f : nf - 1;
         BinCtx b;
+        b.f = fc;
         b.k = fc / nq;
         const int z = fc - b.k * nq;
         b.lo = m.win_lo[b.k];
@@ -474,15 +580,20 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
                 // only the origin on the ray pair: J += 2 w I_bdy (sim_radiation.tpp:243-264)
                 const int bo = m.cell2bdy[o];
                 double I = 0.0;
-                if (bo >= 0) I = planck(m.bdy_T[bo], b.nu_o);
+                if (bo >= 0) I = m.ibdy[(int64_t)bo * nf + fc];
                 else if (lane == 0) atomicAdd(&flags->trace_err, 1ull);
                 Jf += 2.0 * wr * (0.5 * (I + I));
                 continue;
             }
             double u, L;
             sweep<Pol>(m, pol, b, ofr, nfr, obk, nbk, chi_o, t_o, o, flags, u, L);
-            if (Pol::kFallback && !(isfinite(u) && isfinite(L)))
-                fp64_pair(m, t, pol.eps, pol.kap, b, ofr, nfr, obk, nbk, o, flags, u, L);
+            if (Pol::kFallback && !(isfinite(u) && isfinite(L))) {
+                // leave this pair to the double-precision patch pass
+                const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
+                if (slot < (unsigned long long)a.patch_cap) a.patch[slot] = make_int4(o, r, fc, 0);
+                else atomicAdd(&flags->patch_overflow, 1ull);
+                continue;
+            }
             Jf += 2.0 * wr * u;
             Lf += lam_pre * wr * L;
         }
@@ -500,6 +611,127 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
             for (int s = 16; s > 0; s >>= 1) {
                 vj += __shfl_xor_sync(0xffffffffu, vj, s);
                 vl += __shfl_xor_sync(0xffffffffu, vl, s);
+            }
+            if (lane == 0) { sJ[kk] += vj; sL[kk] += vl; }
+        }
+        __syncwarp();
+    }
+    for (int k = lane; k < K; k += 32) {
+        a.Jlin[(int64_t)o * K + k] = sJ[k];
+        a.Lam[(int64_t)o * K + k] = sL[k];
+    }
+}
+
+// The mixed solve with the points of each (ray pair, chunk) staged in
+// shared memory: the warp first gathers every point's record and the
+// scaled opacities of the chunk's (at most two) lines with parallel,
+// coalesced loads, then runs the serial sweep on shared memory only.  Used
+// when the lines' windows do not overlap, every 32-bin chunk spans at most
+// two lines (31 or more bins per line) and ray pairs fit the buffer.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksStaged)
+    formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, StagedMixedPolicy pol,
+                               int cap, DevFlags *flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
+    if (oi >= t.o_count) return;
+    const int o = (int)(t.o_begin + oi);
+    const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
+    StagedPt *pts = reinterpret_cast<StagedPt *>(smem_raw) + (size_t)warp * cap;
+    double *sJ = reinterpret_cast<double *>(reinterpret_cast<StagedPt *>(smem_raw) +
+                                            (size_t)kWarpsPerBlock * cap) + (size_t)warp * 2 * K;
+    double *sL = sJ + K;
+    for (int k = lane; k < K; k += 32) { sJ[k] = 0.0; sL[k] = 0.0; }
+    __syncwarp();
+    const float2 *ek = a.ehat_khat;
+    pol.pts = pts;
+
+    const double pw_o = m.pw[o];
+    const int nchunks = (nf + 31) >> 5;
+    for (int c = 0; c < nchunks; c++) {
+        const int f = c * 32 + lane;
+        const bool active = f < nf;
+        const int fc = active ? f : nf - 1;
+        BinCtx b;
+        b.f = fc;
+        b.k = fc / nq;
+        const int z = fc - b.k * nq;
+        b.lo = b.hi = b.k;
+        const double line_k = m.line[b.k];
+        const double root = m.roots[z];
+        b.nu_o = radd(line_k, rmul(rmul(line_k, pw_o), root));
+        b.q = (float)(pw_o * root);
+        const int k0 = (c * 32) / nq;
+        const int k1 = min(K - 1, k0 + 1);
+        pol.hi = b.k != k0;
+
+        float chi_o, t_o;
+        double chi_o_d;
+        pol.origin(m, o, b, chi_o, t_o, chi_o_d);
+        const double width_o = line_k * pw_o;
+        const double iw = 1.0 / width_o;
+        const double xo = iw * (b.nu_o - line_k);
+        const double prof_o = iw * kINVERSE_SQRT_PI * exp(-(xo * xo));
+        const double lam_pre = m.A[b.k] * (m.qw[z] * 2.0) * (b.nu_o * prof_o / chi_o_d);
+
+        double Jf = 0.0, Lf = 0.0;
+        for (int r = 0; r < m.npairs; r++) {
+            const int ar = m.antipod[r];
+            const double wr = m.ray_w[r];
+            const int64_t ir = (int64_t)r * t.o_count + oi;
+            const int64_t iar = (int64_t)ar * t.o_count + oi;
+            const int nr_ = t.len[ir], nar_ = t.len[iar];
+            const bool rfront = nr_ > nar_;
+            const int64_t ofr = rfront ? t.off[ir] : t.off[iar];
+            const int64_t obk = rfront ? t.off[iar] : t.off[ir];
+            const int nfr = rfront ? nr_ : nar_;
+            const int nbk = rfront ? nar_ : nr_;
+            if (nfr == 0) {
+                const int bo = m.cell2bdy[o];
+                double I = 0.0;
+                if (bo >= 0) I = m.ibdy[(int64_t)bo * nf + fc];
+                else if (lane == 0) atomicAdd(&flags->trace_err, 1ull);
+                Jf += 2.0 * wr * (0.5 * (I + I));
+                continue;
+            }
+            // stage: front points at [0, nfr), back points at [nfr, nfr + nbk)
+            const int np = nfr + nbk;
+            for (int j = lane; j < np; j += 32) {
+                const int64_t gi = j < nfr ? ofr + j : obk + (j - nfr);
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(t.mp) + gi);
+                StagedPt q;
+                q.cell = __float_as_int(v.x);
+                q.delta = v.y;
+                q.dzs = v.z;
+                q.ipw = v.w;
+                q.e0 = __ldg(ek + (unsigned)q.cell * K + k0);
+                q.e1 = __ldg(ek + (unsigned)q.cell * K + k1);
+                pts[j] = q;
+            }
+            __syncwarp();
+            double u, L;
+            sweep<StagedMixedPolicy>(m, pol, b, 0, nfr, nfr, nbk, chi_o, t_o, o, flags, u, L);
+            __syncwarp();
+            if (!(isfinite(u) && isfinite(L))) {
+                const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
+                if (slot < (unsigned long long)a.patch_cap) a.patch[slot] = make_int4(o, r, fc, 0);
+                else atomicAdd(&flags->patch_overflow, 1ull);
+                continue;
+            }
+            Jf += 2.0 * wr * u;
+            Lf += lam_pre * wr * L;
+        }
+        if (a.J && active) a.J[(int64_t)o * nf + f] = Jf;
+        const double jw = active ? m.qw[z] * Jf : 0.0;
+        const double lw = active ? Lf : 0.0;
+        const int klast = min(K - 1, (c * 32 + 31) / nq);
+        for (int kk = k0; kk <= klast; kk++) {
+            double vj = (active && b.k == kk) ? jw : 0.0;
+            double vl = (active && b.k == kk) ? lw : 0.0;
+#pragma unroll
+            for (int sh = 16; sh > 0; sh >>= 1) {
+                vj += __shfl_xor_sync(0xffffffffu, vj, sh);
+                vl += __shfl_xor_sync(0xffffffffu, vl, sh);
             }
             if (lane == 0) { sJ[kk] += vj; sL[kk] += vl; }
         }
@@ -539,9 +771,35 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         pol.kap = a.kap;
         run(pol);
     };
-    if (precision == MGR_MIXED) {
+    const bool staged = precision == MGR_MIXED && !m.overlap && m.nquads >= 31 &&
+                        a.max_pair_points > 0 && a.max_pair_points <= kStagedMaxCap;
+    if (staged) {
+        const int cap = (int)((a.max_pair_points + 1) & ~1);
+        const size_t sm = (size_t)kWarpsPerBlock * cap * sizeof(StagedPt) +
+                          (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
+        cudaError_t e = cudaFuncSetAttribute(formal_solve_staged_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        StagedMixedPolicy pol;
+        pol.pts = nullptr;
+        pol.hi = false;
+        pol.floor_hat = (float)(1.0E-26 * a.mixed_scale);
+        pol.inv_scale = 1.0 / a.mixed_scale;
+        pol.eps = a.eps;
+        pol.kap = a.kap;
+        formal_solve_staged_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, sm, s>>>(m, t, a, pol,
+                                                                                    cap, flags);
+    } else if (precision == MGR_MIXED) {
         if (m.overlap) mixed(MixedPolicy<true>{});
         else mixed(MixedPolicy<false>{});
+    }
+    if (precision == MGR_MIXED) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        // entries beyond patch_cap are counted in DevFlags; the host then
+        // solves again in double
+        const unsigned pblocks = (unsigned)((a.patch_cap + 127) / 128);
+        patch_kernel<<<pblocks, 128, 0, s>>>(m, t, a, flags);
     } else {
         if (m.overlap) fp64(Fp64Policy<true>{});
         else fp64(Fp64Policy<false>{});
