@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--weights", default=os.path.join(ROOT, "magritte_b200", "weights",
                                                       "wind_rotor10.npz"))
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
-    ap.add_argument("--workload", default="wind64", choices=["wind64", "lattice16"])
+    ap.add_argument("--workload", default="wind64", choices=["wind64", "wind32", "lattice16"],
+                    help="wind32 (the same wind at 32^3) is the small case for ncu captures")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -69,12 +70,16 @@ def make_model(name):
     import magritte_b200.model as M
     if name == "wind64":
         return M.config2()
+    if name == "wind32":
+        return M.wind_model(32, seed=2, nlev=10, nside=2, name="wind32")
     return M.config1()
 
 
 def workload_config(name, model, prec, start="LTE"):
-    return {"workload": "64^3 spherical wind, 10-level rotor" if name == "wind64"
-            else "16^3 lattice cloud, 2-level line",
+    names = {"wind64": "64^3 spherical wind, 10-level rotor",
+             "wind32": "32^3 spherical wind, 10-level rotor",
+             "lattice16": "16^3 lattice cloud, 2-level line"}
+    return {"workload": names[name],
             "cells": model.ncells, "levels": model.linedata.nlev, "lines": model.nlines,
             "bins_per_line": model.nquads, "rays": model.nrays,
             "start": start, "tol_max_rel": TOL, "ng": True, "precision": prec,
@@ -193,7 +198,7 @@ def cpu_oracle_time(model, iterations, sample_s, nthreads=None):
 # which cannot afford the full solve on CPU, multiplies its per-iteration
 # time by the count the same algorithm needs (equal iteration counts of
 # the oracle and the device path are checked by the GPU tests).
-REFERENCE_ITERATIONS = {"wind64": 5, "lattice16": None}
+REFERENCE_ITERATIONS = {"wind64": 5, "wind32": None, "lattice16": None}
 
 
 def run_reference(args):
@@ -208,7 +213,7 @@ def run_reference(args):
         if o is not None:
             iters, _ = o.compute_level_populations(True, MAX_ITER, TOL)
         else:
-            iters = 5
+            iters = REFERENCE_ITERATIONS["wind64"]
     cpu = CpuOracle(model)
     for w in range(args.warmup):
         cpu.time(iters, min(2.0, args.cpu_sample_s), seed=100 + w)
