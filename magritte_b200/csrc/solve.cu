@@ -292,66 +292,6 @@ struct MixedPolicy {
     }
 };
 
-// One traced point staged in shared memory for the chunk being solved:
-// the float record plus the scaled opacity pairs of the chunk's two lines.
-struct __align__(16) StagedPt {
-    float delta, dzs, ipw;
-    int cell;
-    float2 e0, e1;
-};
-
-// Mixed precision on points staged in shared memory (no global loads in
-// the sweep).  Indices are positions in the staged buffer.
-struct StagedMixedPolicy {
-    using Real = float;
-    struct Pt {
-        float delta, dzs, ipw;
-        int cell;
-        float2 e;
-    };
-    const StagedPt *pts;
-    bool hi;                  // this lane's bin belongs to the chunk's second line
-    float floor_hat;
-    double inv_scale;
-    const double *eps, *kap;
-
-    __device__ __forceinline__ Pt load(int64_t i) const {
-        const StagedPt &q = pts[i];
-        Pt p;
-        p.delta = q.delta;
-        p.dzs = q.dzs;
-        p.ipw = q.ipw;
-        p.cell = q.cell;
-        p.e = hi ? q.e1 : q.e0;
-        return p;
-    }
-    __device__ __forceinline__ double freq(const Pt &p, const BinCtx &b) const {
-        return (1.0 + (double)p.delta) * b.nu_o;
-    }
-    __device__ __forceinline__ void eval_pt(const ModelView &, const Pt &p, const BinCtx &b,
-                                            float &chi, float &t) const {
-        const float off = fmaf(p.delta, b.q, p.delta + b.q);
-        const float x = off * p.ipw;
-        const float g = fabsf(x) <= 11.0f ? (1.0f + off) * __expf(-x * x) : 0.0f;
-        float eta = p.e.x * g;
-        chi = fmaf(p.e.y, g, floor_hat);
-        if (chi < floor_hat) eta = __int_as_float(0x7fc00000);   // redone in double
-        t = __fdividef(eta, chi);
-    }
-    __device__ __forceinline__ static double dtau(float chi_a, float chi_b, float dzs) {
-        return (double)((chi_a + chi_b) * dzs);
-    }
-    __device__ __forceinline__ static float dz_of(const Pt &p) { return p.dzs; }
-    __device__ __forceinline__ void origin(const ModelView &m, int o, const BinCtx &b,
-                                           float &chi, float &t, double &chi_phys) const {
-        double e64, c64;
-        eta_chi_double(m, eps, kap, o, b.nu_o, b.k, b.k, e64, c64);
-        chi = (float)(c64 * m.mixed_scale);
-        t = (float)(e64 / c64);
-        chi_phys = c64;
-    }
-};
-
 // ------------------------------------------------------------------ chains
 
 // Elimination of one half of the ray pair from its far end toward the origin.
@@ -622,15 +562,186 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     }
 }
 
+// ------------------------------------------------------------------ staged mixed solve
+//
 // The mixed solve with the points of each (ray pair, chunk) staged in
-// shared memory: the warp first gathers every point's record and the
-// scaled opacities of the chunk's (at most two) lines with parallel,
-// coalesced loads, then runs the serial sweep on shared memory only.  Used
+// shared memory.  The warp first gathers every point's record and the
+// scaled opacities of the chunk's (at most two) lines with parallel loads,
+// then each lane runs its serial elimination on shared memory only.  Used
 // when the lines' windows do not overlap, every 32-bin chunk spans at most
 // two lines (31 or more bins per line) and ray pairs fit the buffer.
+//
+// The elimination runs on half optical depths dh = dtau/2 with F~ = F'/2,
+// S~ = S/2, which removes constant factors from the step:
+//     H = dh_far + dh_near, P = H dh_far, Q = H dh_near,
+//     w = Q (P + F~), D = 1/(P + 2w), F~ <- w D, S~ <- (t P + S~) Q D
+// (the same recursion as the generic sweep with p = 2P, q = 2Q).  The
+// boundary row becomes D = 1/(2dh(dh+1)+1), F~ = dh(dh+1)D, S~ = dh(t dh+I)D
+// and the origin row u = (t PQ + S~f Q + S~b P)/(F~f Q + F~b P + PQ),
+// L = PQ/(...) with P, Q built from the two segments at the origin.
+
+// One traced point of the staged pair: the float record and the opacity
+// pairs (eps, kap) * INVSQRTPI / pw * X of the chunk's two lines.  A point
+// whose line opacity is negative carries a NaN emissivity, which sends the
+// (pair, bin) to the double-precision patch pass.
+struct __align__(16) StagedPt {
+    float delta;   // Doppler shift - 1
+    float dzh;     // dZ / (4 X): dh = (chi_a + chi_b) * dzh for chi scaled by X
+    float ipws;    // sqrt(log2 e) / profile width
+    int cell;
+    float2 e[2];
+};
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Scaled opacity and source function of a staged point for a lane whose
+// bin sits q = pw_o * root widths from its line: with off = nu/line - 1,
+// chi X = 1e-26 X + Khat (1 + off) 2^-(off ipws)^2, the profile vanishing
+// (flushed to zero) beyond ~9.3 widths, inside the reference's 11-width cut.
+__device__ __forceinline__ void staged_eval(const StagedPt *p, int eo, float q, float floor_hat,
+                                            float &chi, float &t) {
+    const float4 r = *reinterpret_cast<const float4 *>(p);
+    const float2 e = reinterpret_cast<const float2 *>(p)[eo];
+    const float off = fmaf(r.x, q, r.x + q);
+    const float x = off * r.z;
+    const float g = ex2_approx(-x * x);
+    const float rg = fmaf(off, g, g);
+    chi = fmaf(e.y, rg, floor_hat);
+    t = e.x * rg * rcp_approx(chi);
+}
+
+#ifndef MGR_STAGED_NEWTON
+#define MGR_STAGED_NEWTON 1
+#endif
+// 1/x of the staged elimination: hardware estimate and MGR_STAGED_NEWTON
+// Newton-Raphson refinements.  One refinement leaves an error far below the
+// float rounding of the optical depths (the mixed J and ALO agree with the
+// two-refinement build to the same 6e-8 against FP64 on the 64^3 wind).
+__device__ __forceinline__ double rcp_chain(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#pragma unroll
+    for (int i = 0; i < MGR_STAGED_NEWTON; i++) y = fma(y, fma(-x, y, 1.0), y);
+    return y;
+}
+
+struct HalfChain {
+    float chi_a, t_a, dzh_a;   // current point
+    double dh_prev, F, S;      // scaled Rybicki-Hummer state
+
+    __device__ __forceinline__ void start(float chi, float t, float dzh) {
+        chi_a = chi; t_a = t; dzh_a = dzh;
+    }
+    // boundary row of the far end
+    __device__ __forceinline__ void first(float chi_b, float t_b, float dzh_b, double I) {
+        const double dh = (double)((chi_a + chi_b) * dzh_a);
+        const double dh1 = dh + 1.0;
+        const double D = rcp_chain(fma(2.0 * dh, dh1, 1.0));
+        F = dh * dh1 * D;
+        S = dh * fma((double)t_a, dh, I) * D;
+        dh_prev = dh;
+        chi_a = chi_b; t_a = t_b; dzh_a = dzh_b;
+    }
+    __device__ __forceinline__ void step(float chi_b, float t_b, float dzh_b) {
+        const double dh = (double)((chi_a + chi_b) * dzh_a);
+        const double H = dh_prev + dh;
+        const double P = H * dh_prev, Q = H * dh;
+        const double w = Q * (P + F);
+        const double D = rcp_chain(fma(2.0, w, P));
+        F = w * D;
+        S = fma((double)t_a, P, S) * (Q * D);
+        dh_prev = dh;
+        chi_a = chi_b; t_a = t_b; dzh_a = dzh_b;
+    }
+};
+
+// u and L at the origin for the staged pair: front points at [0, nfr)
+// (far end at nfr-1), back points at [nfr, nfr+nbk).
+__device__ __forceinline__ void staged_sweep(const StagedPt *pts, int nfr, int nbk, int eo,
+                                             float q, float floor_hat, const BdyCtx &bc,
+                                             const BinCtx &b, float chi_o, float t_o,
+                                             const ModelView &m, int origin, DevFlags *flags,
+                                             double &u, double &L) {
+    HalfChain fr, bk;
+    float chi, t;
+    const StagedPt *pf = pts + (nfr - 1);
+    staged_eval(pf, eo, q, floor_hat, chi, t);
+    fr.start(chi, t, pf->dzh);
+    const double I0 = boundary_intensity(bc, (1.0 + (double)pf->delta) * b.nu_o, pf->cell, b.f, flags);
+    if (nfr >= 2) {
+        pf--;
+        staged_eval(pf, eo, q, floor_hat, chi, t);
+        fr.first(chi, t, pf->dzh, I0);
+    } else {
+        fr.first(chi_o, t_o, 0.0f, I0);
+    }
+    double In = 0.0;
+    const StagedPt *pb = pts + (nfr + nbk - 1);
+    if (nbk > 0) {
+        staged_eval(pb, eo, q, floor_hat, chi, t);
+        bk.start(chi, t, pb->dzh);
+        In = boundary_intensity(bc, (1.0 + (double)pb->delta) * b.nu_o, pb->cell, b.f, flags);
+        if (nbk >= 2) {
+            pb--;
+            staged_eval(pb, eo, q, floor_hat, chi, t);
+            bk.first(chi, t, pb->dzh, In);
+        } else {
+            bk.first(chi_o, t_o, 0.0f, In);
+        }
+    } else {
+        const int bo = __ldg(m.cell2bdy + origin);
+        if (bo >= 0) In = __ldg(m.ibdy + (int64_t)bo * m.nfreqs + b.f);
+        else atomicAdd(&flags->trace_err, 1ull);
+    }
+    // both halves have interior points: advance them in lock step
+    const StagedPt *const pb_end = pts + nfr;   // first back point (nearest the origin)
+    const StagedPt *const pf_end = pts;
+    if (nbk >= 2) {
+        while (pb > pb_end) {
+            pf--; pb--;
+            float chi_p, t_p, chi_q, t_q;
+            staged_eval(pf, eo, q, floor_hat, chi_p, t_p);
+            staged_eval(pb, eo, q, floor_hat, chi_q, t_q);
+            fr.step(chi_p, t_p, pf->dzh);
+            bk.step(chi_q, t_q, pb->dzh);
+        }
+        bk.step(chi_o, t_o, 0.0f);
+    }
+    // the rest of the front half
+    while (pf > pf_end) {
+        pf--;
+        staged_eval(pf, eo, q, floor_hat, chi, t);
+        fr.step(chi, t, pf->dzh);
+    }
+    if (nfr >= 2) fr.step(chi_o, t_o, 0.0f);
+
+    const double to = (double)t_o;
+    if (nbk == 0) {
+        const double dh = fr.dh_prev;
+        const double D = rcp_chain(fma(dh, dh + 1.0, fr.F));
+        u = fma(dh, fma(to, dh, In), fr.S) * D;
+        L = dh * dh * D;
+        return;
+    }
+    const double H = fr.dh_prev + bk.dh_prev;
+    const double P = H * fr.dh_prev, Q = H * bk.dh_prev;
+    const double PQ = P * Q;
+    const double D = rcp_chain(fma(fr.F, Q, fma(bk.F, P, PQ)));
+    u = fma(to, PQ, fma(fr.S, Q, bk.S * P)) * D;
+    L = PQ * D;
+}
+
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksStaged)
-    formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, StagedMixedPolicy pol,
-                               int cap, DevFlags *flags) {
+    formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, int cap, DevFlags *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
@@ -644,7 +755,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksStaged)
     for (int k = lane; k < K; k += 32) { sJ[k] = 0.0; sL[k] = 0.0; }
     __syncwarp();
     const float2 *ek = a.ehat_khat;
-    pol.pts = pts;
+    const BdyCtx bc = bdy_ctx(m);
+    const float floor_hat = (float)(1.0E-26 * a.mixed_scale);
+    const float kSqrtLog2e = 1.2011224087864498f;
 
     const double pw_o = m.pw[o];
     const int nchunks = (nf + 31) >> 5;
@@ -663,16 +776,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksStaged)
         b.q = (float)(pw_o * root);
         const int k0 = (c * 32) / nq;
         const int k1 = min(K - 1, k0 + 1);
-        pol.hi = b.k != k0;
+        const int eo = b.k != k0 ? 3 : 2;   // float2 index of this lane's line in a StagedPt
 
-        float chi_o, t_o;
-        double chi_o_d;
-        pol.origin(m, o, b, chi_o, t_o, chi_o_d);
+        // origin in double; a negative line opacity there poisons the bin
+        double e64, c64;
+        eta_chi_double(m, a.eps, a.kap, o, b.nu_o, b.k, b.k, e64, c64);
+        const float chi_o = (float)(c64 * m.mixed_scale);
+        const float t_o = c64 < 1.0E-26 ? __int_as_float(0x7fc00000) : (float)(e64 / c64);
         const double width_o = line_k * pw_o;
         const double iw = 1.0 / width_o;
         const double xo = iw * (b.nu_o - line_k);
         const double prof_o = iw * kINVERSE_SQRT_PI * exp(-(xo * xo));
-        const double lam_pre = m.A[b.k] * (m.qw[z] * 2.0) * (b.nu_o * prof_o / chi_o_d);
+        const double lam_pre = m.A[b.k] * (m.qw[z] * 2.0) * (b.nu_o * prof_o / c64);
 
         double Jf = 0.0, Lf = 0.0;
         for (int r = 0; r < m.npairs; r++) {
@@ -694,23 +809,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksStaged)
                 Jf += 2.0 * wr * (0.5 * (I + I));
                 continue;
             }
-            // stage: front points at [0, nfr), back points at [nfr, nfr + nbk)
             const int np = nfr + nbk;
             for (int j = lane; j < np; j += 32) {
                 const int64_t gi = j < nfr ? ofr + j : obk + (j - nfr);
                 const float4 v = __ldg(reinterpret_cast<const float4 *>(t.mp) + gi);
-                StagedPt q;
-                q.cell = __float_as_int(v.x);
-                q.delta = v.y;
-                q.dzs = v.z;
-                q.ipw = v.w;
-                q.e0 = __ldg(ek + (unsigned)q.cell * K + k0);
-                q.e1 = __ldg(ek + (unsigned)q.cell * K + k1);
-                pts[j] = q;
+                const unsigned cell = (unsigned)__float_as_int(v.x);
+                float2 e0 = __ldg(ek + cell * K + k0);
+                float2 e1 = __ldg(ek + cell * K + k1);
+                if (e0.y < 0.0f) e0.x = __int_as_float(0x7fc00000);
+                if (e1.y < 0.0f) e1.x = __int_as_float(0x7fc00000);
+                float4 *dst = reinterpret_cast<float4 *>(pts + j);
+                dst[0] = make_float4(v.y, 0.5f * v.z, v.w * kSqrtLog2e, v.x);
+                dst[1] = make_float4(e0.x, e0.y, e1.x, e1.y);
             }
             __syncwarp();
             double u, L;
-            sweep<StagedMixedPolicy>(m, pol, b, 0, nfr, nfr, nbk, chi_o, t_o, o, flags, u, L);
+            staged_sweep(pts, nfr, nbk, eo, b.q, floor_hat, bc, b, chi_o, t_o, m, o, flags, u, L);
             __syncwarp();
             if (!(isfinite(u) && isfinite(L))) {
                 const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
@@ -780,15 +894,8 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         cudaError_t e = cudaFuncSetAttribute(formal_solve_staged_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        StagedMixedPolicy pol;
-        pol.pts = nullptr;
-        pol.hi = false;
-        pol.floor_hat = (float)(1.0E-26 * a.mixed_scale);
-        pol.inv_scale = 1.0 / a.mixed_scale;
-        pol.eps = a.eps;
-        pol.kap = a.kap;
-        formal_solve_staged_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, sm, s>>>(m, t, a, pol,
-                                                                                    cap, flags);
+        formal_solve_staged_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, sm, s>>>(m, t, a, cap,
+                                                                                    flags);
     } else if (precision == MGR_MIXED) {
         if (m.overlap) mixed(MixedPolicy<true>{});
         else mixed(MixedPolicy<false>{});
