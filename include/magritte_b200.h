@@ -301,6 +301,48 @@ mgr_status mgr_mlp_loss_grad(int device, const mgr_mlp *net, const float *X, con
 
 /* --- without allocation ------------------------------------------------- */
 
+/* --- batches of independent models ------------------------------------- */
+
+/* Declares the uploaded point cloud to be the union of `nseg` independent
+ * models that share species, rays and quadrature and whose neighbour graphs
+ * are disjoint: model s owns cells [seg_begin[s], seg_begin[s+1]) with
+ * seg_begin[0] = 0 and seg_begin[nseg] = ncells (nseg+1 entries).
+ * mgr_compute_level_populations then iterates every model to its own
+ * convergence: statistics and Ng coefficients per model, and a model that
+ * has converged is frozen (populations kept, its origins skipped by the
+ * formal solve).  The reference runs one Simulation per model
+ * (Simulation::compute_level_populations, sim_lines.tpp:61-164, per model);
+ * no single reference function corresponds.  nseg = 1 returns to the
+ * single-model path.  Cleared by mgr_upload_model. */
+mgr_status mgr_set_segments(mgr_handle *h, int64_t nseg, const int64_t *seg_begin);
+
+/* After mgr_compute_level_populations on a batch: stats[3*s .. 3*s+2] =
+ * fraction not converged, mean and max relative population change of model
+ * s at its last iteration; iterations[s] = the iteration at which model s
+ * converged (the total when it did not).  Either pointer may be NULL.
+ * No reference counterpart. */
+mgr_status mgr_get_segment_results(mgr_handle *h, double *stats, int64_t *iterations);
+
+/* --- autotuning of the formal solve -------------------------------------- */
+
+/* Which formal-solve kernel ran and with what block shape.  No reference
+ * counterpart. */
+typedef struct {
+    int32_t kernel;           /* 0 generic, 1 staged (shared-memory) mixed kernel, -1 none yet */
+    int32_t min_blocks;       /* resident blocks per SM it is compiled for */
+    int32_t warps_per_block;
+    int32_t tuned;            /* 1 once every candidate has been timed */
+    float ms[8];              /* time of each candidate's solve (0: not timed) */
+} mgr_tuning;
+
+/* With enable != 0 the next formal solves of each precision each run one of
+ * the compiled candidates (register budgets for 6, 7 and 8 resident blocks
+ * per SM), timed with CUDA events; every later solve uses the fastest.  The
+ * candidates compute identical results.  Tuning restarts after a retrace.
+ * No reference counterpart. */
+mgr_status mgr_set_autotune(mgr_handle *h, int32_t enable);
+mgr_status mgr_get_tuning(mgr_handle *h, int32_t precision, mgr_tuning *out);
+
 /* Largest ncells * nlev that mgr_convergence_noalloc accepts. */
 #define MGR_NOALLOC_MAX_ELEMENTS 67108864LL
 

@@ -37,6 +37,7 @@ EXPORTS = (
     "mgr_synchronize", "mgr_timer_start", "mgr_timer_stop", "mgr_get_launch_count",
     "mgr_convergence_noalloc", "mgr_mlp_param_count", "mgr_get_features", "mgr_get_lte_logfrac",
     "mgr_warm_start", "mgr_mlp_train", "mgr_mlp_forward", "mgr_mlp_loss_grad",
+    "mgr_set_segments", "mgr_get_segment_results", "mgr_set_autotune", "mgr_get_tuning",
 )
 MLP_FEATURES = 10
 MLP_HIDDEN = 128
@@ -79,6 +80,11 @@ class TrainOpts(C.Structure):
 class AliOpts(C.Structure):
     _fields_ = [("use_ng", _i32), ("precision", _i32), ("max_iter", _i64),
                 ("tol_max_rel", _dbl), ("use_graph", _i32), ("reserved", _i32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("kernel", _i32), ("min_blocks", _i32), ("warps_per_block", _i32),
+                ("tuned", _i32), ("ms", C.c_float * 8)]
 
 
 class MagritteError(RuntimeError):
@@ -138,6 +144,10 @@ def load(build_if_missing: bool = True):
     L.mgr_mlp_train.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _P, _P, _i64, C.POINTER(TrainOpts), _P]
     L.mgr_mlp_forward.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _i64, _P]
     L.mgr_mlp_loss_grad.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _P, _P, _i64, _P, _P]
+    L.mgr_set_segments.argtypes = [_P, _i64, _P]
+    L.mgr_get_segment_results.argtypes = [_P, _P, _P]
+    L.mgr_set_autotune.argtypes = [_P, _i32]
+    L.mgr_get_tuning.argtypes = [_P, _i32, C.POINTER(Tuning)]
     _lib = L
     return L
 

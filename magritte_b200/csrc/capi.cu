@@ -96,8 +96,35 @@ struct mgr_handle {
     double *ibdy = nullptr;            // [nboundary][nfreqs]
     int4 *patch = nullptr;             // mixed solve: entries redone in double
     unsigned long long *patch_count = nullptr;
+    unsigned long long *h_patch = nullptr;   // pinned copy of patch_count
     int64_t patch_cap = 0;
     int64_t last_patched = 0;
+
+    // batch of independent models (nseg > 0)
+    int64_t nseg = 0;
+    int64_t *seg_begin_d = nullptr;
+    int32_t *cell_seg_d = nullptr, *seg_active_d = nullptr;
+    double *seg_stats_d = nullptr;
+    double *h_seg_stats = nullptr;     // pinned [3*nseg]
+    int32_t *h_seg_active = nullptr;   // pinned [nseg]
+    std::vector<int64_t> seg_iters;
+
+    // online autotuner of the formal solve: per precision, the first solves
+    // each run one compiled variant; later solves use the fastest
+    bool autotune = false;
+    struct Tune {
+        int next = 0, best = -1, kind = -1;
+        float ms[kSolveVariants] = {};
+    } tune[2];
+
+    // CUDA graphs of the ALI iteration (rebuilt when gen or the key changes)
+    int64_t gen = 0;
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        int64_t gen = -1;
+        int key = 0;
+        int kernels = 0;   // kernels per replay
+    } g_solve, g_level, g_ng;
 };
 
 namespace {
@@ -137,9 +164,38 @@ void free_traces(mgr_handle *h) {
     h->bcap = 0;
     h->traced = false;
     h->stored = false;
+    h->gen++;
+}
+
+void free_graph(mgr_handle::Graph &g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    g.gen = -1;
+}
+
+void free_segments(mgr_handle *h) {
+    free_ptr((void *&)h->seg_begin_d);
+    free_ptr((void *&)h->cell_seg_d);
+    free_ptr((void *&)h->seg_active_d);
+    free_ptr((void *&)h->seg_stats_d);
+    if (h->h_seg_stats) cudaFreeHost(h->h_seg_stats);
+    if (h->h_seg_active) cudaFreeHost(h->h_seg_active);
+    h->h_seg_stats = nullptr;
+    h->h_seg_active = nullptr;
+    h->nseg = 0;
+    h->seg_iters.clear();
+    h->mv.nseg = 0;
+    h->mv.seg_begin = nullptr;
+    h->mv.cell_seg = nullptr;
+    h->mv.seg_active = nullptr;
+    h->gen++;
 }
 
 void free_model(mgr_handle *h) {
+    free_graph(h->g_solve);
+    free_graph(h->g_level);
+    free_graph(h->g_ng);
+    free_segments(h);
     free_traces(h);
     free_ptr((void *&)h->len_all);
     for (void *p : h->model_allocs) cudaFree(p);
@@ -159,11 +215,9 @@ void reset_flags(mgr_handle *h) {
     ck(cudaMemsetAsync(h->flags, 0, sizeof(DevFlags), h->stream), "reset flags");
 }
 
-// Reads the device error counters; returns the status they imply.
-void check_flags(mgr_handle *h, const char *what) {
-    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream),
-       "read flags");
-    ck(cudaStreamSynchronize(h->stream), what);
+// Raises the status that the device error counters (already copied to the
+// pinned host copy) imply.
+void check_flags_copied(mgr_handle *h, const char *what) {
     const DevFlags &f = *h->h_flags;
     if (f.trace_err || f.stuck_err)
         fail(MGR_ERR_TRACE, std::string(what) + ": " + std::to_string(f.trace_err + f.stuck_err) +
@@ -175,6 +229,14 @@ void check_flags(mgr_handle *h, const char *what) {
     if (f.lu_err)
         fail(MGR_ERR_LU_SINGULAR, std::string(what) + ": zero pivot in the rate equations of " +
                                       std::to_string(f.lu_err) + " cell(s)");
+}
+
+// Reads the device error counters; raises the status they imply.
+void check_flags(mgr_handle *h, const char *what) {
+    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream),
+       "read flags");
+    ck(cudaStreamSynchronize(h->stream), what);
+    check_flags_copied(h, what);
 }
 
 LevelArgs level_args(mgr_handle *h) {
@@ -485,6 +547,8 @@ void do_trace(mgr_handle *h) {
     need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
     set_device(h);
     free_traces(h);
+    h->tune[0] = mgr_handle::Tune{};   // the kernel choice depends on the trace
+    h->tune[1] = mgr_handle::Tune{};
     const int64_t N = h->N, R = h->nrays, n = R * N;
     h->max_pair_points = 0;
     if (!h->len_all) h->len_all = dalloc<int32_t>(h, n, nullptr);
@@ -579,19 +643,9 @@ void boundary_table(mgr_handle *h) {
     h->bdy_set = true;
 }
 
-void do_solve(mgr_handle *h, int precision) {
-    need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
-    need(h->pops_valid, MGR_ERR_STATE, "no level populations yet (LTE or set_populations)");
-    need(precision == MGR_FP64 || precision == MGR_MIXED, MGR_ERR_INVALID_ARG, "bad precision");
-    set_device(h);
-    if (!h->traced) do_trace(h);
-    if (!h->bdy_set) boundary_table(h);
-    if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
-    if (precision == MGR_MIXED && !h->patch) {
-        h->patch_cap = 1 << 20;
-        h->patch = dalloc<int4>(h, h->patch_cap, nullptr);
-        h->patch_count = dalloc<unsigned long long>(h, 1, nullptr);
-    }
+void do_solve(mgr_handle *h, int precision, bool use_graph);
+
+SolveArgs solve_args(mgr_handle *h) {
     SolveArgs a{};
     a.eps = h->eps;
     a.kap = h->kap;
@@ -604,45 +658,156 @@ void do_solve(mgr_handle *h, int precision) {
     a.patch_count = h->patch_count;
     a.patch_cap = h->patch_cap;
     a.max_pair_points = h->max_pair_points;
-    reset_flags(h);
-    unsigned long long patched = 0;
-    auto launch = [&](const TraceView &t) {
-        if (precision == MGR_MIXED)
-            ck(cudaMemsetAsync(h->patch_count, 0, sizeof(unsigned long long), h->stream), "patch reset");
-        ck(launch_formal_solve(h->mv, t, a, precision, h->flags, h->stream), "formal solve");
-        h->launches += precision == MGR_MIXED ? 2 : 1;
-        if (precision == MGR_MIXED) {
-            unsigned long long c = 0;
-            ck(cudaMemcpyAsync(&c, h->patch_count, sizeof(c), cudaMemcpyDeviceToHost, h->stream), "d2h");
-            ck(cudaStreamSynchronize(h->stream), "patch count");
-            patched += c;
-        }
-    };
-    ck(cudaEventRecord(h->ev0, h->stream), "event");
-    if (h->stored) {
-        TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
-        launch(t);
-    } else {
-        for (int64_t o0 = 0; o0 < h->N; o0 += h->batch_origins) {
-            const int64_t cnt = std::min(h->batch_origins, h->N - o0);
-            TraceView t = build_batch(h, o0, cnt);
-            launch(t);
-        }
+    return a;
+}
+
+void solve_prepare(mgr_handle *h, int precision) {
+    need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
+    need(h->pops_valid, MGR_ERR_STATE, "no level populations yet (LTE or set_populations)");
+    need(precision == MGR_FP64 || precision == MGR_MIXED, MGR_ERR_INVALID_ARG, "bad precision");
+    set_device(h);
+    if (!h->traced) do_trace(h);
+    if (!h->bdy_set) boundary_table(h);
+    if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
+    if (precision == MGR_MIXED && !h->patch) {
+        h->patch_cap = 1 << 20;
+        h->patch = dalloc<int4>(h, h->patch_cap, nullptr);
+        h->patch_count = dalloc<unsigned long long>(h, 1, nullptr);
+        h->gen++;
     }
-    ck(cudaEventRecord(h->ev1, h->stream), "event");
-    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream), "flags");
-    ck(cudaStreamSynchronize(h->stream), "solve sync");
+}
+
+// The compiled variant for the next solve: a candidate still to be timed
+// while autotuning, else the fastest timed one, else the default (-1).
+int solve_variant(mgr_handle *h, int precision, bool *timing) {
+    mgr_handle::Tune &tu = h->tune[precision == MGR_MIXED];
+    *timing = false;
+    if (tu.best >= 0) return tu.best;
+    if (h->autotune && tu.next < kSolveVariants) {
+        *timing = true;
+        return tu.next;
+    }
+    return -1;
+}
+
+void tune_record(mgr_handle *h, int precision, int variant, float ms) {
+    mgr_handle::Tune &tu = h->tune[precision == MGR_MIXED];
+    tu.ms[variant] = ms;
+    tu.next = variant + 1;
+    if (tu.next == kSolveVariants) {
+        int best = 0;
+        for (int v = 1; v < kSolveVariants; v++)
+            if (tu.ms[v] < tu.ms[best]) best = v;
+        tu.best = best;
+    }
+}
+
+// Enqueues one formal solve over the stored trace (asynchronous, capturable).
+int enqueue_stored_solve(mgr_handle *h, int precision, int variant) {
+    const SolveArgs a = solve_args(h);
+    reset_flags(h);
+    if (precision == MGR_MIXED)
+        ck(cudaMemsetAsync(h->patch_count, 0, sizeof(unsigned long long), h->stream), "patch reset");
+    TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
+    int kind = 0;
+    ck(launch_formal_solve(h->mv, t, a, precision, variant, h->flags, h->stream, &kind),
+       "formal solve");
+    h->tune[precision == MGR_MIXED].kind = kind;
+    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream),
+       "flags");
+    if (precision == MGR_MIXED)
+        ck(cudaMemcpyAsync(h->h_patch, h->patch_count, sizeof(unsigned long long),
+                           cudaMemcpyDeviceToHost, h->stream), "patch count");
+    return precision == MGR_MIXED ? 2 : 1;
+}
+
+// Runs `body` (stream work only; returns the kernels it launches) through a
+// CUDA graph captured on first use and replayed while neither the handle's
+// generation nor `key` changed.  Returns the kernels per replay.
+int graph_run(mgr_handle *h, mgr_handle::Graph &g, int key, const std::function<int()> &body) {
+    if (!g.exec || g.gen != h->gen || g.key != key) {
+        free_graph(g);
+        ck(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed), "begin capture");
+        cudaGraph_t graph = nullptr;
+        try {
+            g.kernels = body();
+        } catch (...) {
+            cudaStreamEndCapture(h->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        ck(cudaStreamEndCapture(h->stream, &graph), "end capture");
+        const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        ck(e, "graph instantiate");
+        g.gen = h->gen;
+        g.key = key;
+    }
+    ck(cudaGraphLaunch(g.exec, h->stream), "graph launch");
+    return g.kernels;
+}
+
+void finish_solve(mgr_handle *h, int precision, int variant, bool timing, int64_t patched) {
     if (precision == MGR_MIXED && h->h_flags->patch_overflow) {
         // more float failures than the patch list holds: solve in double
-        do_solve(h, MGR_FP64);
+        do_solve(h, MGR_FP64, false);
         return;
     }
     check_flags(h, "formal solve");
     float ms = 0.f;
     ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+    if (timing) tune_record(h, precision, variant, ms);
     h->last_solve_ms = ms;
     h->last_updates = h->updates_per_solve;
-    h->last_patched = (int64_t)patched;
+    h->last_patched = patched;
+}
+
+void do_solve(mgr_handle *h, int precision, bool use_graph) {
+    solve_prepare(h, precision);
+    bool timing = false;
+    const int variant = solve_variant(h, precision, &timing);
+    if (h->stored) {
+        // the events stay outside the graph (a captured record only orders work)
+        ck(cudaEventRecord(h->ev0, h->stream), "event");
+        if (use_graph && !timing) {
+            const int key = precision * 16 + (variant + 1) * 2 + (h->keep_J ? 1 : 0);
+            h->launches += graph_run(h, h->g_solve, key,
+                                     [&] { return enqueue_stored_solve(h, precision, variant); });
+        } else {
+            h->launches += enqueue_stored_solve(h, precision, variant);
+        }
+        ck(cudaEventRecord(h->ev1, h->stream), "event");
+        ck(cudaStreamSynchronize(h->stream), "solve sync");
+        finish_solve(h, precision, variant, timing,
+                     precision == MGR_MIXED ? (int64_t)*h->h_patch : 0);
+        return;
+    }
+    // traces in batches of origins, rebuilt for every solve
+    const SolveArgs a = solve_args(h);
+    reset_flags(h);
+    unsigned long long patched = 0;
+    ck(cudaEventRecord(h->ev0, h->stream), "event");
+    for (int64_t o0 = 0; o0 < h->N; o0 += h->batch_origins) {
+        const int64_t cnt = std::min(h->batch_origins, h->N - o0);
+        TraceView t = build_batch(h, o0, cnt);
+        if (precision == MGR_MIXED)
+            ck(cudaMemsetAsync(h->patch_count, 0, sizeof(unsigned long long), h->stream), "patch reset");
+        int kind = 0;
+        ck(launch_formal_solve(h->mv, t, a, precision, variant, h->flags, h->stream, &kind),
+           "formal solve");
+        h->tune[precision == MGR_MIXED].kind = kind;
+        h->launches += precision == MGR_MIXED ? 2 : 1;
+        if (precision == MGR_MIXED) {
+            ck(cudaMemcpyAsync(h->h_patch, h->patch_count, sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, h->stream), "d2h");
+            ck(cudaStreamSynchronize(h->stream), "patch count");
+            patched += *h->h_patch;
+        }
+    }
+    ck(cudaEventRecord(h->ev1, h->stream), "event");
+    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream), "flags");
+    ck(cudaStreamSynchronize(h->stream), "solve sync");
+    finish_solve(h, precision, variant, timing, (int64_t)patched);
 }
 
 void read_stats(mgr_handle *h) {
@@ -650,23 +815,65 @@ void read_stats(mgr_handle *h) {
     ck(cudaStreamSynchronize(h->stream), "stats sync");
 }
 
+// Convergence statistics (and per-model ones for a batch) and the error
+// counters, copied to pinned host memory.  Stream work only.
+int enqueue_stats(mgr_handle *h, const LevelArgs &a) {
+    int n = 0;
+    if (h->nseg > 0) {
+        ck(launch_seg_convergence(h->mv, a, h->seg_stats_d, h->stream), "model convergence");
+        ck(cudaMemcpyAsync(h->h_seg_stats, h->seg_stats_d, 3 * h->nseg * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream), "model stats");
+        n = 1;
+    }
+    ck(cudaMemcpyAsync(h->h_stats, h->stats, 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+       "stats");
+    ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream),
+       "flags");
+    return n;
+}
+
+// Statistical equilibrium (+ statistics); returns the kernels launched.
+int enqueue_stateq(mgr_handle *h) {
+    const LevelArgs a = level_args(h);
+    reset_flags(h);
+    ck(launch_stateq(h->mv, a, h->flags, h->stream), "stateq");
+    return 2 + enqueue_stats(h, a);
+}
+
+// Jeff, statistical equilibrium and statistics after a formal solve.
+int enqueue_level(mgr_handle *h) {
+    ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
+    return 1 + enqueue_stateq(h);
+}
+
+// Ng step, its convergence statistics and the new emissivities/opacities.
+int enqueue_ng(mgr_handle *h) {
+    const LevelArgs a = level_args(h);
+    reset_flags(h);
+    int n = 0;
+    if (h->nseg > 0) {
+        ck(launch_seg_ng(h->mv, a, h->stream), "model ng");
+        n += 1;
+    } else {
+        ck(launch_ng(h->mv, a, h->stream), "ng");
+        n += 3;
+    }
+    ck(launch_convergence(h->mv, a, h->stream), "convergence");
+    ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
+    return n + 3 + enqueue_stats(h, a);
+}
+
 void do_stateq(mgr_handle *h) {
     need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
-    reset_flags(h);
-    ck(launch_stateq(h->mv, level_args(h), h->flags, h->stream), "stateq");
-    h->launches += 2;
-    check_flags(h, "statistical equilibrium");
-    read_stats(h);
+    h->launches += enqueue_stateq(h);
+    ck(cudaStreamSynchronize(h->stream), "statistical equilibrium");
+    check_flags_copied(h, "statistical equilibrium");
 }
 
 void do_ng(mgr_handle *h) {
     need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
-    const LevelArgs a = level_args(h);
-    ck(launch_ng(h->mv, a, h->stream), "ng");
-    ck(launch_convergence(h->mv, a, h->stream), "convergence");
-    ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
-    h->launches += 6;
-    read_stats(h);
+    h->launches += enqueue_ng(h);
+    ck(cudaStreamSynchronize(h->stream), "ng");
 }
 
 }  // namespace
@@ -714,6 +921,7 @@ mgr_status mgr_create(int device, mgr_handle **out) {
         ck(cudaEventCreate(&h->tev1), "event");
         ck(cudaMallocHost(&h->h_stats, 8 * sizeof(double)), "pinned");
         ck(cudaMallocHost(&h->h_flags, sizeof(DevFlags)), "pinned");
+        ck(cudaMallocHost(&h->h_patch, sizeof(unsigned long long)), "pinned");
     });
     if (s != MGR_OK) {
         mgr_destroy(h);
@@ -730,6 +938,7 @@ mgr_status mgr_destroy(mgr_handle *h) {
     free_model(h);
     if (h->h_stats) cudaFreeHost(h->h_stats);
     if (h->h_flags) cudaFreeHost(h->h_flags);
+    if (h->h_patch) cudaFreeHost(h->h_patch);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->tev0) cudaEventDestroy(h->tev0);
@@ -852,7 +1061,7 @@ mgr_status mgr_set_keep_J(mgr_handle *h, int32_t keep) {
 }
 
 mgr_status mgr_compute_radiation_field(mgr_handle *h, int32_t precision) {
-    return run(h, [&] { do_solve(h, precision); });
+    return run(h, [&] { do_solve(h, precision, false); });
 }
 
 mgr_status mgr_compute_Jeff(mgr_handle *h) {
@@ -889,23 +1098,66 @@ mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts
         need(opts->max_iter >= 1, MGR_ERR_INVALID_ARG, "max_iter must be >= 1");
         need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
         need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+        const bool graph = opts->use_graph != 0;
+        auto converged = [&](double fnc, double mx) {
+            return opts->tol_max_rel > 0.0 ? mx < opts->tol_max_rel : !(fnc > 0.005);
+        };
+        if (h->nseg > 0) {
+            for (int64_t g = 0; g < h->nseg; g++) h->h_seg_active[g] = 1;
+            std::fill(h->seg_iters.begin(), h->seg_iters.end(), (int64_t)0);
+            ck(cudaMemcpyAsync(h->seg_active_d, h->h_seg_active, h->nseg * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, h->stream), "model mask");
+        }
         int64_t iteration = 0, normal = 0;
         bool more = true;
         while (more && iteration < opts->max_iter) {
             iteration++;
             if (opts->use_ng && normal == 4) {
-                do_ng(h);
+                h->launches += graph ? graph_run(h, h->g_ng, 0, [&] { return enqueue_ng(h); })
+                                     : enqueue_ng(h);
+                ck(cudaStreamSynchronize(h->stream), "ng");
                 normal = 0;
             } else {
-                do_solve(h, opts->precision);
-                ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
-                h->launches += 1;
-                do_stateq(h);
+                do_solve(h, opts->precision, graph);
+                h->launches += graph ? graph_run(h, h->g_level, 0, [&] { return enqueue_level(h); })
+                                     : enqueue_level(h);
+                ck(cudaStreamSynchronize(h->stream), "statistical equilibrium");
+                check_flags_copied(h, "statistical equilibrium");
                 normal++;
             }
-            const double fnc = h->h_stats[0], mx = h->h_stats[2];
+            double mx = h->h_stats[2];
+            if (h->nseg > 0) {
+                bool any = false, changed = false;
+                mx = 0.0;
+                for (int64_t g = 0; g < h->nseg; g++) {
+                    if (!h->h_seg_active[g]) continue;
+                    const double *st = h->h_seg_stats + 3 * g;
+                    mx = std::max(mx, st[2]);
+                    if (converged(st[0], st[2])) {
+                        h->h_seg_active[g] = 0;
+                        h->seg_iters[g] = iteration;
+                        changed = true;
+                    } else {
+                        any = true;
+                    }
+                }
+                if (changed)
+                    ck(cudaMemcpyAsync(h->seg_active_d, h->h_seg_active, h->nseg * sizeof(int32_t),
+                                       cudaMemcpyHostToDevice, h->stream), "model mask");
+                more = any;
+            } else {
+                more = !converged(h->h_stats[0], mx);
+            }
             if (err_max_hist) err_max_hist[iteration - 1] = mx;
-            more = opts->tol_max_rel > 0.0 ? !(mx < opts->tol_max_rel) : (fnc > 0.005);
+        }
+        if (h->nseg > 0) {
+            for (int64_t g = 0; g < h->nseg; g++)
+                if (h->h_seg_active[g]) h->seg_iters[g] = iteration;
+            // leave every model active for later single steps
+            for (int64_t g = 0; g < h->nseg; g++) h->h_seg_active[g] = 1;
+            ck(cudaMemcpyAsync(h->seg_active_d, h->h_seg_active, h->nseg * sizeof(int32_t),
+                               cudaMemcpyHostToDevice, h->stream), "model mask");
+            ck(cudaStreamSynchronize(h->stream), "model mask");
         }
         if (iterations) *iterations = iteration;
         not_converged = more;
@@ -913,6 +1165,75 @@ mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts
     });
     if (s == MGR_OK && not_converged) return MGR_ERR_NOT_CONVERGED;
     return s;
+}
+
+mgr_status mgr_set_segments(mgr_handle *h, int64_t nseg, const int64_t *seg_begin) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        need(nseg >= 1 && seg_begin != nullptr, MGR_ERR_INVALID_ARG, "need nseg >= 1 and bounds");
+        need(seg_begin[0] == 0 && seg_begin[nseg] == h->N, MGR_ERR_INVALID_ARG,
+             "model bounds must start at 0 and end at ncells");
+        for (int64_t g = 0; g < nseg; g++)
+            need(seg_begin[g + 1] > seg_begin[g], MGR_ERR_INVALID_ARG, "empty or unordered model");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        free_segments(h);
+        if (nseg == 1) return;
+        std::vector<int32_t> cs(h->N);
+        for (int64_t g = 0; g < nseg; g++)
+            for (int64_t c = seg_begin[g]; c < seg_begin[g + 1]; c++) cs[c] = (int32_t)g;
+        h->seg_begin_d = upload<int64_t>(h, seg_begin, nseg + 1, nullptr);
+        h->cell_seg_d = upload<int32_t>(h, cs.data(), h->N, nullptr);
+        h->seg_active_d = dalloc<int32_t>(h, nseg, nullptr);
+        h->seg_stats_d = dalloc<double>(h, 3 * nseg, nullptr);
+        ck(cudaMemset(h->seg_stats_d, 0, 3 * nseg * sizeof(double)), "memset");
+        ck(cudaMallocHost(&h->h_seg_stats, 3 * nseg * sizeof(double)), "pinned");
+        ck(cudaMallocHost(&h->h_seg_active, nseg * sizeof(int32_t)), "pinned");
+        for (int64_t g = 0; g < nseg; g++) h->h_seg_active[g] = 1;
+        ck(cudaMemcpy(h->seg_active_d, h->h_seg_active, nseg * sizeof(int32_t),
+                      cudaMemcpyHostToDevice), "upload");
+        h->nseg = nseg;
+        h->seg_iters.assign(nseg, 0);
+        h->mv.nseg = nseg;
+        h->mv.seg_begin = h->seg_begin_d;
+        h->mv.cell_seg = h->cell_seg_d;
+        h->mv.seg_active = h->seg_active_d;
+    });
+}
+
+mgr_status mgr_get_segment_results(mgr_handle *h, double *stats, int64_t *iterations) {
+    return run(h, [&] {
+        need(h->nseg > 0, MGR_ERR_STATE, "no model batch set");
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        if (stats)
+            ck(cudaMemcpy(stats, h->seg_stats_d, 3 * h->nseg * sizeof(double),
+                          cudaMemcpyDeviceToHost), "d2h");
+        if (iterations)
+            for (int64_t g = 0; g < h->nseg; g++) iterations[g] = h->seg_iters[g];
+    });
+}
+
+mgr_status mgr_set_autotune(mgr_handle *h, int32_t enable) {
+    return run(h, [&] {
+        h->autotune = enable != 0;
+        h->tune[0] = mgr_handle::Tune{};
+        h->tune[1] = mgr_handle::Tune{};
+    });
+}
+
+mgr_status mgr_get_tuning(mgr_handle *h, int32_t precision, mgr_tuning *out) {
+    return run(h, [&] {
+        need(out != nullptr, MGR_ERR_INVALID_ARG, "NULL output");
+        need(precision == MGR_FP64 || precision == MGR_MIXED, MGR_ERR_INVALID_ARG, "bad precision");
+        const mgr_handle::Tune &tu = h->tune[precision == MGR_MIXED];
+        *out = mgr_tuning{};
+        out->kernel = tu.kind;
+        const int v = tu.best >= 0 ? tu.best : (tu.kind == 1 ? 2 : 1);
+        out->min_blocks = solve_variant_blocks(v);
+        out->warps_per_block = 4;
+        out->tuned = tu.best >= 0 ? 1 : 0;
+        for (int i = 0; i < kSolveVariants && i < 8; i++) out->ms[i] = tu.ms[i];
+    });
 }
 
 mgr_status mgr_set_populations(mgr_handle *h, const double *pop) {

@@ -114,7 +114,8 @@ __global__ void __launch_bounds__(kStateqWarps * 32) stateq_kernel(ModelView m, 
     __shared__ double red[kStateqWarps * 3];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t p = (int64_t)blockIdx.x * kStateqWarps + warp;
-    const bool valid = p < m.N;
+    // cells of a converged model of a batch keep their populations
+    const bool valid = p < m.N && !(m.seg_active && !m.seg_active[m.cell_seg[p]]);
     const int nl = m.nlev, K = m.nrad, last = nl - 1;
     double *M = Msh[warp];
     double *y = ysh[warp];

@@ -92,6 +92,11 @@ struct ModelView {
     double pop_prec;
     double mixed_scale;    // X: power of two scaling the float opacities
     int overlap;           // some line window holds more than its own line
+    // batches of independent models (nullptr / 0 for a single model)
+    int64_t nseg;
+    const int64_t *seg_begin;   // [nseg+1] first cell of each model
+    const int32_t *cell_seg;    // [N] model of each cell
+    const int32_t *seg_active;  // [nseg] 1 while the model iterates
 };
 
 // One traced point in the mixed-precision format (one 16-byte load).
@@ -143,8 +148,14 @@ struct SolveArgs {
     unsigned long long *patch_count;
     int64_t patch_cap;
 };
+// Formal solve of the origins of one trace store.  variant selects the
+// register budget (one of kSolveVariants compiled resident-block counts;
+// < 0: the default); *kind receives 1 when the staged mixed kernel ran.
+constexpr int kSolveVariants = 3;
 cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const SolveArgs &a,
-                                int precision, DevFlags *flags, cudaStream_t s);
+                                int precision, int variant, DevFlags *flags, cudaStream_t s,
+                                int *kind);
+int solve_variant_blocks(int variant);
 
 struct LevelArgs {
     double *pop, *prev1, *prev2, *prev3;   // [N*nlev]
@@ -165,6 +176,11 @@ cudaError_t launch_stateq(const ModelView &m, const LevelArgs &a, DevFlags *flag
 cudaError_t launch_convergence(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_ng(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 int level_partials_needed(const ModelView &m);
+// Per-model convergence statistics (3 per model: fraction not converged,
+// mean and max relative change) and per-model Ng steps, for batches.
+cudaError_t launch_seg_convergence(const ModelView &m, const LevelArgs &a, double *seg_stats,
+                                   cudaStream_t s);
+cudaError_t launch_seg_ng(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 
 // Warm-start network on the device (pointers into one parameter buffer).
 struct MlpDevice {

@@ -44,14 +44,11 @@ namespace mgr {
 namespace {
 
 constexpr int kWarpsPerBlock = 4;
-#ifndef MGR_SOLVE_MIN_BLOCKS
-#define MGR_SOLVE_MIN_BLOCKS 7
-#endif
-constexpr int kMinBlocks = MGR_SOLVE_MIN_BLOCKS;   // 7: 28 warps per SM (measured best of 4..8)
-#ifndef MGR_STAGED_MIN_BLOCKS
-#define MGR_STAGED_MIN_BLOCKS 8
-#endif
-constexpr int kMinBlocksStaged = MGR_STAGED_MIN_BLOCKS;
+// Resident blocks per SM each solve kernel is compiled for (its register
+// budget): the autotuner's candidates.  Defaults when not tuning: 7 for the
+// generic kernel, 8 for the staged one (measured best on the 64^3 wind).
+constexpr int kVariantBlocks[kSolveVariants] = {6, 7, 8};
+constexpr int kDefaultGeneric = 1, kDefaultStaged = 2;
 #ifndef MGR_STAGED_MAX_POINTS
 #define MGR_STAGED_MAX_POINTS 768
 #endif
@@ -87,41 +84,42 @@ struct BdyCtx {
 };
 
 // Radiation::rescale_I_bdy (scalar build, Model/Radiation/radiation.tpp:341-373)
-// on the table of Simulation::compute_boundary_intensities.  The grid of
-// cell p is ascending, so the reference's linear notch search (first bin with
-// freq <= nu_p) is found by stepping from the lane's own bin f0, which is
-// within a few bins of the answer for Doppler shifts of a few widths.
-__device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p, int f0,
-                                                  DevFlags *flags) {
+// on the table of Simulation::compute_boundary_intensities.  The reference
+// takes the first bin of cell p's grid with freq <= nu_p(f) by a linear
+// search; the grid ascends (lines do not interleave, which the spectral
+// discretisation checks), so the same bin is found by bisection: first the
+// line whose last bin is >= freq, then the bin within that line.
+__device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p, DevFlags *flags) {
     const int b = __ldg(c.cell2bdy + p);
     if (b < 0) {
         atomicAdd(&flags->trace_err, 1ull);
         return 0.0;
     }
     const double pwp = __ldg(c.pw + p);
-    const int nq = c.nq, nf = c.nf;
-    auto nu_at = [&](int f) {
-        const int k = f / nq;
+    const int nq = c.nq, nf = c.nf, K = nf / nq;
+    auto nu_kz = [&](int k, int z) {
         const double line = __ldg(c.line + k);
-        return radd(line, rmul(rmul(line, pwp), __ldg(c.roots + (f - k * nq))));
+        return radd(line, rmul(rmul(line, pwp), __ldg(c.roots + z)));
     };
-    int f = f0;
-    int steps = 0;
-    while (f < nf && !(freq <= nu_at(f)) && steps < 16) { f++; steps++; }
-    while (f > 0 && freq <= nu_at(f - 1) && steps < 16) { f--; steps++; }
-    if (steps >= 16) {   // far from the hint: bisect
-        int lo = 0, hi = nf;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (freq <= nu_at(mid)) hi = mid;
-            else lo = mid + 1;
-        }
-        f = lo;
+    int lo = 0, hi = K;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (freq <= nu_kz(mid, nq - 1)) hi = mid;
+        else lo = mid + 1;
     }
-    const int notch = f < nf ? f : nf - 1;
     const double *I = c.ibdy + (int64_t)b * nf;
+    if (lo == K) return __ldg(I + nf - 1);   // above the grid
+    const int k = lo;
+    int zl = 0, zh = nq - 1;
+    while (zl < zh) {
+        const int mid = (zl + zh) >> 1;
+        if (freq <= nu_kz(k, mid)) zh = mid;
+        else zl = mid + 1;
+    }
+    const int notch = k * nq + zl;
     if (notch == 0 || notch == nf - 1) return __ldg(I + notch);
-    const double nu1 = nu_at(notch), nu2 = nu_at(notch - 1);
+    const double nu1 = nu_kz(k, zl);
+    const double nu2 = zl > 0 ? nu_kz(k, zl - 1) : nu_kz(k - 1, nq - 1);
     const double I1 = __ldg(I + notch), I2 = __ldg(I + notch - 1);
     return (I2 - I1) / (nu2 - nu1) * (freq - nu1) + I1;
 }
@@ -346,7 +344,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
         const auto p = pol.load(ofr + nfr - 1);
         pol.eval_pt(m, p, b, chi, t);
         fr.chi_a = chi; fr.t_a = t; fr.dz_a = Pol::dz_of(p);
-        I0 = boundary_intensity(bc, pol.freq(p, b), p.cell, b.f, flags);
+        I0 = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
     }
     if (nfr >= 2) {
         const auto p = pol.load(ofr + nfr - 2);
@@ -360,7 +358,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
         const auto p = pol.load(obk + nbk - 1);
         pol.eval_pt(m, p, b, chi, t);
         bk.chi_a = chi; bk.t_a = t; bk.dz_a = Pol::dz_of(p);
-        In = boundary_intensity(bc, pol.freq(p, b), p.cell, b.f, flags);
+        In = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
         if (nbk >= 2) {
             const auto q = pol.load(obk + nbk - 2);
             pol.eval_pt(m, q, b, chi, t);
@@ -460,7 +458,7 @@ __global__ void patch_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *fl
     if (a.J) atomicAdd(a.J + (int64_t)o * nf + f, 2.0 * wr * u);
 }
 
-template <class Pol>
+template <class Pol, int kMinBlocks>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     formal_solve_kernel(ModelView m, TraceView t, SolveArgs a, Pol pol, DevFlags *flags) {
     using Real = typename Pol::Real;
@@ -469,6 +467,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
     if (oi >= t.o_count) return;
     const int o = (int)(t.o_begin + oi);
+    if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
     double *sJ = smem + (size_t)warp * 2 * K;
     double *sL = sJ + K;
@@ -676,7 +675,7 @@ __device__ __forceinline__ void staged_sweep(const StagedPt *pts, int nfr, int n
     const StagedPt *pf = pts + (nfr - 1);
     staged_eval(pf, eo, q, floor_hat, chi, t);
     fr.start(chi, t, pf->dzh);
-    const double I0 = boundary_intensity(bc, (1.0 + (double)pf->delta) * b.nu_o, pf->cell, b.f, flags);
+    const double I0 = boundary_intensity(bc, (1.0 + (double)pf->delta) * b.nu_o, pf->cell, flags);
     if (nfr >= 2) {
         pf--;
         staged_eval(pf, eo, q, floor_hat, chi, t);
@@ -689,7 +688,7 @@ __device__ __forceinline__ void staged_sweep(const StagedPt *pts, int nfr, int n
     if (nbk > 0) {
         staged_eval(pb, eo, q, floor_hat, chi, t);
         bk.start(chi, t, pb->dzh);
-        In = boundary_intensity(bc, (1.0 + (double)pb->delta) * b.nu_o, pb->cell, b.f, flags);
+        In = boundary_intensity(bc, (1.0 + (double)pb->delta) * b.nu_o, pb->cell, flags);
         if (nbk >= 2) {
             pb--;
             staged_eval(pb, eo, q, floor_hat, chi, t);
@@ -703,10 +702,10 @@ __device__ __forceinline__ void staged_sweep(const StagedPt *pts, int nfr, int n
         else atomicAdd(&flags->trace_err, 1ull);
     }
     // both halves have interior points: advance them in lock step
-    const StagedPt *const pb_end = pts + nfr;   // first back point (nearest the origin)
-    const StagedPt *const pf_end = pts;
     if (nbk >= 2) {
-        while (pb > pb_end) {
+        const int nlock = nbk - 2;
+#pragma unroll 2
+        for (int i = 0; i < nlock; i++) {
             pf--; pb--;
             float chi_p, t_p, chi_q, t_q;
             staged_eval(pf, eo, q, floor_hat, chi_p, t_p);
@@ -717,7 +716,9 @@ __device__ __forceinline__ void staged_sweep(const StagedPt *pts, int nfr, int n
         bk.step(chi_o, t_o, 0.0f);
     }
     // the rest of the front half
-    while (pf > pf_end) {
+    const int nrest = (int)(pf - pts);
+#pragma unroll 2
+    for (int i = 0; i < nrest; i++) {
         pf--;
         staged_eval(pf, eo, q, floor_hat, chi, t);
         fr.step(chi, t, pf->dzh);
@@ -740,13 +741,15 @@ __device__ __forceinline__ void staged_sweep(const StagedPt *pts, int nfr, int n
     L = PQ * D;
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksStaged)
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, int cap, DevFlags *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
     if (oi >= t.o_count) return;
     const int o = (int)(t.o_begin + oi);
+    if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
     StagedPt *pts = reinterpret_cast<StagedPt *>(smem_raw) + (size_t)warp * cap;
     double *sJ = reinterpret_cast<double *>(reinterpret_cast<StagedPt *>(smem_raw) +
@@ -860,13 +863,25 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocksStaged)
 }  // namespace
 
 cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const SolveArgs &a,
-                                int precision, DevFlags *flags, cudaStream_t s) {
+                                int precision, int variant, DevFlags *flags, cudaStream_t s,
+                                int *kind) {
     if (t.o_count == 0) return cudaSuccess;
     const int64_t blocks = (t.o_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const size_t shmem = (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
+    const bool staged = precision == MGR_MIXED && !m.overlap && m.nquads >= 31 &&
+                        a.max_pair_points > 0 && a.max_pair_points <= kStagedMaxCap;
+    if (kind) *kind = staged ? 1 : 0;
+    if (variant < 0 || variant >= kSolveVariants) variant = staged ? kDefaultStaged : kDefaultGeneric;
     auto run = [&](auto pol) {
-        formal_solve_kernel<decltype(pol)>
-            <<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, pol, flags);
+        using P = decltype(pol);
+        auto go = [&](auto kern) {
+            kern<<<(unsigned)blocks, kWarpsPerBlock * 32, shmem, s>>>(m, t, a, pol, flags);
+        };
+        switch (variant) {
+            case 0: go(formal_solve_kernel<P, kVariantBlocks[0]>); break;
+            case 1: go(formal_solve_kernel<P, kVariantBlocks[1]>); break;
+            default: go(formal_solve_kernel<P, kVariantBlocks[2]>); break;
+        }
     };
     auto mixed = [&](auto pol) {
         pol.mp = t.mp;
@@ -885,17 +900,24 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         pol.kap = a.kap;
         run(pol);
     };
-    const bool staged = precision == MGR_MIXED && !m.overlap && m.nquads >= 31 &&
-                        a.max_pair_points > 0 && a.max_pair_points <= kStagedMaxCap;
     if (staged) {
         const int cap = (int)((a.max_pair_points + 1) & ~1);
         const size_t sm = (size_t)kWarpsPerBlock * cap * sizeof(StagedPt) +
                           (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
-        cudaError_t e = cudaFuncSetAttribute(formal_solve_staged_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        auto go = [&](auto kern) -> cudaError_t {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)sm);
+            if (e != cudaSuccess) return e;
+            kern<<<(unsigned)blocks, kWarpsPerBlock * 32, sm, s>>>(m, t, a, cap, flags);
+            return cudaSuccess;
+        };
+        cudaError_t e;
+        switch (variant) {
+            case 0: e = go(formal_solve_staged_kernel<kVariantBlocks[0]>); break;
+            case 1: e = go(formal_solve_staged_kernel<kVariantBlocks[1]>); break;
+            default: e = go(formal_solve_staged_kernel<kVariantBlocks[2]>); break;
+        }
         if (e != cudaSuccess) return e;
-        formal_solve_staged_kernel<<<(unsigned)blocks, kWarpsPerBlock * 32, sm, s>>>(m, t, a, cap,
-                                                                                    flags);
     } else if (precision == MGR_MIXED) {
         if (m.overlap) mixed(MixedPolicy<true>{});
         else mixed(MixedPolicy<false>{});
@@ -912,6 +934,10 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         else fp64(Fp64Policy<false>{});
     }
     return cudaGetLastError();
+}
+
+int solve_variant_blocks(int variant) {
+    return variant >= 0 && variant < kSolveVariants ? kVariantBlocks[variant] : 0;
 }
 
 }  // namespace mgr

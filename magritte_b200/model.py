@@ -419,11 +419,14 @@ def wind_model(n: int = 64, L: float = 1.0e13, seed: int = 2, nlev: int = 10,
                rho0: float = 1.0e14, T0: float = 1000.0, vmax: float = 15.0e3,
                x_abund: float = 1.0e-4, vturb: float = 150.0, nside: int = 2,
                npairs: Optional[int] = None, nquads: int = 31, jitter: float = 0.3,
-               name: Optional[str] = None) -> Model:
+               name: Optional[str] = None, species_seed: Optional[int] = None,
+               ray_seed: Optional[int] = None) -> Model:
     """Jittered n^3 grid shaped as a spherical wind: n(H2) = rho0 (r/0.05L)^-2,
     T = T0 (r/0.05L)^-0.7 (both held at their r = 0.05L value inside), radial
     velocity rising linearly to vmax at the half-diagonal; linear rotor with
-    ``nlev`` levels. HEALPix rays (``nside``) unless ``npairs`` is given."""
+    ``nlev`` levels. HEALPix rays (``nside``) unless ``npairs`` is given.
+    The species' collision rates and the antipodal ray set are drawn with
+    ``species_seed`` / ``ray_seed`` (default: ``seed``)."""
     pos, offs, nbr, b2c = lattice_grid(n, L, jitter=jitter, seed=seed)
     c = 0.5 * L
     d = pos - c
@@ -439,11 +442,11 @@ def wind_model(n: int = 64, L: float = 1.0e13, seed: int = 2, nlev: int = 10,
     if npairs is None:
         rays = healpix_nest_vectors(nside)
     else:
-        rays = antipodal_ray_set(npairs, seed)
+        rays = antipodal_ray_set(npairs, seed if ray_seed is None else ray_seed)
     w = np.full(rays.shape[0], 1.0 / rays.shape[0])
     return _assemble(pos, offs, nbr, b2c, vel, T, vturb, n_h2, x_abund,
-                     linear_rotor_species(nlev, seed=seed), rays, w, nquads,
-                     name or f"wind_{n}",
+                     linear_rotor_species(nlev, seed=seed if species_seed is None else species_seed),
+                     rays, w, nquads, name or f"wind_{n}",
                      dict(kind="wind", n=n, L=L, seed=seed, nlev=nlev, rho0=rho0, T0=T0,
                           vmax=vmax, x_abund=x_abund, vturb=vturb, nside=nside,
                           npairs=npairs, jitter=jitter))
@@ -522,7 +525,8 @@ def config3() -> Model:
 
 def config4_member(m: int) -> Model:
     """Member m of the 256-model batch: 2k..60k points, random density scale,
-    T0 and vmax, 20-level rotor, 24 rays (12 antipodal pairs)."""
+    T0 and vmax, 20-level rotor, 24 rays (12 antipodal pairs).  Species and
+    ray set are common to the batch (drawn with seed 4)."""
     rng = np.random.default_rng(4 + m)
     u = rng.uniform()
     N = min(int(2.0e3 * 30.0 ** u), 60000)
@@ -531,7 +535,63 @@ def config4_member(m: int) -> Model:
     T0 = rng.uniform(100.0, 2000.0)
     vmax = rng.uniform(5.0e3, 30.0e3)
     return wind_model(n, seed=4 + m, nlev=20, rho0=rho0, T0=T0, vmax=vmax, npairs=12,
-                      name=f"cfg4_m{m}")
+                      name=f"cfg4_m{m}", species_seed=4, ray_seed=4)
+
+
+def concat_models(models: List[Model], name: str = "batch") -> Model:
+    """One point cloud holding independent models side by side: cells,
+    neighbour lists and boundary cells are renumbered, the graphs stay
+    disjoint, and ``meta["segments"]`` holds each model's first cell (plus
+    the total), which the library uses to iterate every model to its own
+    convergence.  The models must share species, rays, quadrature and
+    population precision."""
+    m0 = models[0]
+    for m in models[1:]:
+        if not (np.array_equal(m.rays, m0.rays) and np.array_equal(m.ray_weights, m0.ray_weights)
+                and np.array_equal(m.quad_roots, m0.quad_roots)
+                and np.array_equal(m.quad_weights, m0.quad_weights)
+                and m.pop_prec == m0.pop_prec and m.max_width_fraction == m0.max_width_fraction
+                and _same_species(m.linedata, m0.linedata)):
+            raise ValueError(f"model {m.name} does not share species/rays/quadrature with {m0.name}")
+    seg = np.zeros(len(models) + 1, dtype=np.int64)
+    seg[1:] = np.cumsum([m.ncells for m in models])
+    offs, nbrs, b2c = [np.zeros(1, dtype=np.int64)], [], []
+    for m, c0 in zip(models, seg[:-1]):
+        offs.append(m.nbr_offsets[1:] + offs[-1][-1])
+        nbrs.append(m.nbr_list + c0)
+        b2c.append(m.boundary2cell + c0)
+    cat = lambda f: np.concatenate([getattr(m, f) for m in models])
+    return Model(position=cat("position"), velocity=cat("velocity"),
+                 nbr_offsets=np.concatenate(offs), nbr_list=np.concatenate(nbrs),
+                 boundary2cell=np.concatenate(b2c), boundary_temperature=cat("boundary_temperature"),
+                 rays=m0.rays, ray_weights=m0.ray_weights, temperature=cat("temperature"),
+                 vturb2=cat("vturb2"), abundance=cat("abundance"), linedata=m0.linedata,
+                 quad_roots=m0.quad_roots, quad_weights=m0.quad_weights, pop_prec=m0.pop_prec,
+                 max_width_fraction=m0.max_width_fraction, name=name,
+                 meta=dict(kind="batch", members=[m.name for m in models],
+                           segments=seg.tolist())).contiguous()
+
+
+def _same_species(a: Linedata, b: Linedata) -> bool:
+    if not (a.num == b.num and a.inverse_mass == b.inverse_mass and len(a.colpar) == len(b.colpar)):
+        return False
+    for f in ("energy", "weight", "irad", "jrad", "A"):
+        if not np.array_equal(getattr(a, f), getattr(b, f)):
+            return False
+    for ca, cb in zip(a.colpar, b.colpar):
+        for f in dataclasses.fields(ca):
+            va, vb = getattr(ca, f.name), getattr(cb, f.name)
+            if isinstance(va, np.ndarray):
+                if not np.array_equal(va, vb):
+                    return False
+            elif va != vb:
+                return False
+    return True
+
+
+def config4(nmodels: int = 256) -> Model:
+    """The 256-model batch as one point cloud of independent models."""
+    return concat_models([config4_member(m) for m in range(nmodels)], name=f"cfg4_batch{nmodels}")
 
 
 def config5() -> Model:

@@ -74,6 +74,10 @@ class Simulation:
         desc, keep = _capi.make_desc(model)
         self._ck(self._lib.mgr_upload_model(self._h, C.byref(desc)))
         self.model = model
+        seg = model.meta.get("segments") if isinstance(model.meta, dict) else None
+        if seg is not None and len(seg) > 2:
+            b = np.ascontiguousarray(seg, dtype=np.int64)
+            self._ck(self._lib.mgr_set_segments(self._h, b.shape[0] - 1, _capi.ptr(b)))
         return 0
 
     def set_trace_budget(self, nbytes: int):
@@ -106,16 +110,20 @@ class Simulation:
         self._record()
 
     def compute_level_populations(self, use_Ng: bool = True, max_niterations: int = 1000,
-                                  precision="fp64", tol_max_rel: float = 0.0) -> int:
+                                  precision="fp64", tol_max_rel: float = 0.0,
+                                  use_graph: bool = False) -> int:
         """ALI loop (``Simulation::compute_level_populations``,
         ``sim_lines.tpp:61-164``); returns the iteration count.
-        ``tol_max_rel`` > 0 stops at max relative population change < tol."""
+        ``tol_max_rel`` > 0 stops at max relative population change < tol;
+        ``use_graph`` replays each iteration's launches as CUDA graphs.  For
+        a batch of models every model iterates to its own convergence and
+        the count is the batch's (``segment_results`` has each model's)."""
         o = _capi.AliOpts()
         o.use_ng = int(bool(use_Ng))
         o.precision = _PREC[precision]
         o.max_iter = int(max_niterations)
         o.tol_max_rel = float(tol_max_rel)
-        o.use_graph = 0
+        o.use_graph = int(bool(use_graph))
         it = C.c_int64(0)
         hist = np.zeros(max(1, int(max_niterations)))
         st = self._ck(self._lib.mgr_compute_level_populations(self._h, C.byref(o), C.byref(it),
@@ -123,6 +131,27 @@ class Simulation:
         self.error_max = list(hist[: it.value])
         self.converged = (st == 0)
         return int(it.value)
+
+    # ------------------------------------------------------ model batches
+    def segment_results(self):
+        """Per-model (fraction not converged, mean, max relative change) at
+        each model's last iteration, and the iteration it converged at."""
+        n = len(self.model.meta["segments"]) - 1
+        st = np.zeros((n, 3))
+        it = np.zeros(n, dtype=np.int64)
+        self._ck(self._lib.mgr_get_segment_results(self._h, _capi.ptr(st), _capi.ptr(it)))
+        return st, it
+
+    # ------------------------------------------------------------ tuning
+    def set_autotune(self, enable: bool = True):
+        self._ck(self._lib.mgr_set_autotune(self._h, int(bool(enable))))
+
+    def tuning(self, precision="mixed") -> dict:
+        t = _capi.Tuning()
+        self._ck(self._lib.mgr_get_tuning(self._h, _PREC[precision], C.byref(t)))
+        return {"kernel": {-1: None, 0: "generic", 1: "staged"}[t.kernel],
+                "min_blocks": t.min_blocks, "warps_per_block": t.warps_per_block,
+                "tuned": bool(t.tuned), "ms": [float(x) for x in t.ms[:3]]}
 
     def get_npoints_on_rays_comoving(self) -> np.ndarray:
         m = self.model

@@ -362,3 +362,25 @@ def test_ali_oracle_converges_and_is_stationary():
     o.compute_Jeff()
     o.compute_level_populations_from_stateq()
     assert np.max(np.abs(o.pop - pop) / pop) < 1e-7
+
+
+def test_concat_models_keeps_each_member():
+    """A batch renumbers cells, neighbours and boundary cells; every member's
+    rays trace exactly as in the member alone (graphs stay disjoint)."""
+    ms = [M.wind_model(n, seed=40 + i, nlev=4, npairs=3, name=f"m{i}", species_seed=40,
+                       ray_seed=40) for i, n in enumerate((4, 5))]
+    b = M.concat_models(ms)
+    seg = b.meta["segments"]
+    assert seg == [0, 64, 64 + 125]
+    assert b.ncells == 189 and b.nboundary == ms[0].nboundary + ms[1].nboundary
+    ob = oracle.Oracle(b).setup()
+    for s, m in enumerate(ms):
+        om = oracle.Oracle(m).setup()
+        for o in (0, m.ncells // 2, m.ncells - 1):
+            for r in range(m.nrays):
+                cm, shm, dzm = om.trace_ray(o, r)
+                cb, shb, dzb = ob.trace_ray(o + seg[s], r)
+                assert np.array_equal(cb, cm + seg[s])
+                assert np.array_equal(shb, shm) and np.array_equal(dzb, dzm)
+    with pytest.raises(ValueError):
+        M.concat_models([ms[0], M.wind_model(4, seed=9, nlev=4, npairs=3)])
