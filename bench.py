@@ -46,6 +46,7 @@ METRIC = "ALI iters & wall-clock to 1e-4 pops on 1 B200: learned+FP32 vs plain F
 TOL = 1.0e-4
 MAX_ITER = 400
 FALLBACK_HBM_GBS = 6650.0
+STAGED_DRAM_BYTES_PER_UPDATE = 0.535
 
 
 def parse():
@@ -56,34 +57,57 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--start", default="learned", choices=["learned", "lte"])
-    ap.add_argument("--weights", default=os.path.join(ROOT, "magritte_b200", "weights",
-                                                      "wind_rotor10.npz"))
+    ap.add_argument("--weights", default=None,
+                    help="warm-start network (default: the workload's trained network)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
-    ap.add_argument("--workload", default="wind64", choices=["wind64", "wind32", "lattice16"],
+    ap.add_argument("--workload", default="wind64", choices=sorted(WORKLOADS),
                     help="wind32 (the same wind at 32^3) is the small case for ncu captures")
+    ap.add_argument("--no-graph", action="store_true", help="launch iterations without CUDA graphs")
+    ap.add_argument("--no-autotune", action="store_true", help="default solve kernel shapes")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
+WEIGHTS_DIR = os.path.join(ROOT, "magritte_b200", "weights")
+# name: (description, builder, trained warm-start network or None)
+WORKLOADS = {
+    "wind64": ("64^3 spherical wind, 10-level rotor", "config2", "wind_rotor10.npz"),
+    "wind32": ("32^3 spherical wind, 10-level rotor", "wind32", "wind_rotor10.npz"),
+    "lattice16": ("16^3 lattice cloud, 2-level line", "config1", None),
+    "batch256": ("256 independent spherical winds of 2k-60k points, 20-level rotor, 24 rays",
+                 "config4", None),
+    "turb128": ("128^3 turbulent cloud, 21-level rotor, 96 rays, 41 bins/line", "config5",
+                "turb_rotor21.npz"),
+}
+
+
 def make_model(name):
     import magritte_b200.model as M
-    if name == "wind64":
-        return M.config2()
-    if name == "wind32":
+    b = WORKLOADS[name][1]
+    if b == "wind32":
         return M.wind_model(32, seed=2, nlev=10, nside=2, name="wind32")
-    return M.config1()
+    return getattr(M, b)()
+
+
+def weights_for(name, override=None):
+    w = override or WORKLOADS[name][2]
+    if w is None:
+        return None
+    p = w if os.path.isabs(w) else os.path.join(WEIGHTS_DIR, w)
+    return p if os.path.exists(p) else None
 
 
 def workload_config(name, model, prec, start="LTE"):
-    names = {"wind64": "64^3 spherical wind, 10-level rotor",
-             "wind32": "32^3 spherical wind, 10-level rotor",
-             "lattice16": "16^3 lattice cloud, 2-level line"}
-    return {"workload": names[name],
-            "cells": model.ncells, "levels": model.linedata.nlev, "lines": model.nlines,
-            "bins_per_line": model.nquads, "rays": model.nrays,
-            "start": start, "tol_max_rel": TOL, "ng": True, "precision": prec,
-            "l2": "inputs larger than L2 (ray traces of several GB re-read every iteration)"}
+    cfg = {"workload": WORKLOADS[name][0],
+           "cells": model.ncells, "levels": model.linedata.nlev, "lines": model.nlines,
+           "bins_per_line": model.nquads, "rays": model.nrays,
+           "start": start, "tol_max_rel": TOL, "ng": True, "precision": prec,
+           "l2": "inputs larger than L2 (ray traces of several GB re-read every iteration)"}
+    seg = model.meta.get("segments")
+    if seg:
+        cfg["models"] = len(seg) - 1
+    return cfg
 
 
 def dist_env():
@@ -198,7 +222,8 @@ def cpu_oracle_time(model, iterations, sample_s, nthreads=None):
 # which cannot afford the full solve on CPU, multiplies its per-iteration
 # time by the count the same algorithm needs (equal iteration counts of
 # the oracle and the device path are checked by the GPU tests).
-REFERENCE_ITERATIONS = {"wind64": 5, "wind32": None, "lattice16": None}
+REFERENCE_ITERATIONS = {"wind64": 5, "wind32": None, "lattice16": None, "batch256": None,
+                        "turb128": None}
 
 
 def run_reference(args):
@@ -255,9 +280,16 @@ def run_b200(args):
     model = make_model(args.workload)
     prec = args.precision
     net = None
+    start_name = "LTE"
     if args.start == "learned":
         from magritte_b200.learned import WarmStartNet
-        net = WarmStartNet.load(args.weights)
+        wp = weights_for(args.workload, args.weights)
+        if wp is not None:
+            net = WarmStartNet.load(wp)
+            if net.nlev != model.linedata.nlev:
+                net = None
+        start_name = "learned" if net is not None else "LTE (no trained network for this species)"
+    graph = not args.no_graph
 
     def start(sim, learned):
         if learned:
@@ -268,14 +300,23 @@ def run_b200(args):
     def one_solve(sim, learned=net is not None, precision=prec):
         sim.trace()
         start(sim, learned)
-        return sim.compute_level_populations(True, MAX_ITER, precision, tol_max_rel=TOL)
+        return sim.compute_level_populations(True, MAX_ITER, precision, tol_max_rel=TOL,
+                                             use_graph=graph)
 
     # ---- device-resident solve
     sim = Simulation(model, device=local if dist else 0)
+    if not args.no_autotune:
+        sim.set_autotune(True)
     sim.compute_spectral_discretisation()
     sim.compute_boundary_intensities()
     for _ in range(args.warmup):
         one_solve(sim)
+    if not args.no_plain:
+        # tune the FP64 kernel before the plain solve is timed
+        sim.trace()
+        start(sim, False)
+        for _ in range(3):
+            sim.compute_radiation_field("fp64")
     if dist:
         tdist.barrier()
     launches0 = sim.launch_count()
@@ -291,6 +332,13 @@ def run_b200(args):
             solve_upd.append(up)
     launches = (sim.launch_count() - launches0) // max(1, args.steps)
     converged = bool(getattr(sim, "converged", False))
+    model_iters = None
+    if model.meta.get("segments"):
+        import numpy as np
+        _, mit = sim.segment_results()
+        model_iters = {"min": int(mit.min()), "median": float(np.median(mit)),
+                       "max": int(mit.max()), "sum": int(mit.sum())}
+    tuning = sim.tuning(prec) if not args.no_autotune else None
     err_hist = list(sim.error_max)
     t_step = statistics.mean(times)
 
@@ -304,7 +352,9 @@ def run_b200(args):
         s2.compute_spectral_discretisation()
         s2.compute_boundary_intensities()
         start(s2, net is not None)
-        s2.compute_level_populations(True, MAX_ITER, prec, tol_max_rel=TOL)
+        if not args.no_autotune:
+            s2.set_autotune(True)
+        s2.compute_level_populations(True, MAX_ITER, prec, tol_max_rel=TOL, use_graph=graph)
         pop = s2.population
         e2e.append(time.perf_counter() - t0)
         s2.close()
@@ -318,6 +368,13 @@ def run_b200(args):
         t_p = sim.timer_stop() / 1e3
         plain = {"start": "LTE", "precision": "fp64", "ali_iterations": it_p, "seconds": t_p,
                  "converged": bool(getattr(sim, "converged", False))}
+        if model.meta.get("segments"):
+            import numpy as np
+            _, mit = sim.segment_results()
+            plain["model_iterations"] = {"min": int(mit.min()), "median": float(np.median(mit)),
+                                         "max": int(mit.max()), "sum": int(mit.sum())}
+        plain["iterations_ratio"] = it_p / max(1, iters[-1])
+        plain["wallclock_ratio"] = t_p / max(1e-12, statistics.mean(times))
     sim.close()
 
     # ---- multi-GPU: max over ranks
@@ -336,22 +393,32 @@ def run_b200(args):
     bpu = 44.0 if prec == "fp64" else 24.0
     avg_ms = statistics.mean(solve_ms)
     achieved = solve_upd[-1] * bpu / (avg_ms / 1e3) / 1e9
+    # DRAM bytes per update of the staged mixed kernel from one ncu capture
+    # of the 32^3 wind (profiles/formal_solve_staged_wind32.md), scaled to
+    # this launch by its update count (same bins per chunk, same ratio)
+    traffic = (solve_upd[-1] * STAGED_DRAM_BYTES_PER_UPDATE
+               if prec == "mixed" and tuning and tuning.get("kernel") == "staged" else None)
     line = {
         "metric": METRIC, "value": t_step / world, "unit": "s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == "fp64" else "f32+f64",
         "data": "synthetic (seeded)",
-        "config": workload_config(args.workload, model, prec, args.start),
+        "config": workload_config(args.workload, model, prec, start_name),
         "ali_iterations": iters[-1], "converged": converged,
+        "model_iterations": model_iters,
+        "solve_kernel": tuning,
         "plain_fp64_lte": plain,
         "final_max_rel_change": err_hist[-1] if err_hist else None,
         "formal_solve": {"ms": avg_ms, "updates": solve_upd[-1],
                          "updates_per_s": solve_upd[-1] / (avg_ms / 1e3)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "note": f"formal-solve kernel; {bpu:.0f} B/update algorithmic; peak "
-                             f"{kind} copy bandwidth"},
+                     "frac": achieved / hbm, "traffic": traffic,
+                     "note": f"formal-solve kernel; effective operand bytes {bpu:.0f} B/update "
+                             f"(what an unstaged kernel reads); peak = {kind} copy bandwidth. The "
+                             f"staged kernel reads each point once per 32 bins: DRAM traffic is "
+                             f"`traffic` bytes per launch, and the kernel is bound by instruction "
+                             f"issue and the XU pipe, not HBM"},
         "e2e": {"value": e2e_t / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),

@@ -335,10 +335,13 @@ typedef struct {
     float ms[8];              /* time of each candidate's solve (0: not timed) */
 } mgr_tuning;
 
-/* With enable != 0 the next formal solves of each precision each run one of
+/* With mode 1 or 2 the next formal solves of each precision each run one of
  * the compiled candidates (register budgets for 6, 7 and 8 resident blocks
- * per SM), timed with CUDA events; every later solve uses the fastest.  The
- * candidates compute identical results.  Tuning restarts after a retrace.
+ * per SM), timed with CUDA events; every later solve uses the fastest.  Mode
+ * 1 first reuses a result that another handle of this process found for the
+ * same device, precision and problem shape; mode 2 always re-times.  The
+ * candidates compute identical results.  Tuning restarts when a retrace
+ * changes the longest ray pair.  Mode 0 (default) turns tuning off.
  * No reference counterpart. */
 mgr_status mgr_set_autotune(mgr_handle *h, int32_t enable);
 mgr_status mgr_get_tuning(mgr_handle *h, int32_t precision, mgr_tuning *out);

@@ -11,6 +11,8 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <mutex>
 #include <limits>
 #include <memory>
 #include <stdexcept>
@@ -111,7 +113,7 @@ struct mgr_handle {
 
     // online autotuner of the formal solve: per precision, the first solves
     // each run one compiled variant; later solves use the fastest
-    bool autotune = false;
+    int autotune = 0;   // 0 off, 1 tune (reuse this process's results), 2 always re-time
     struct Tune {
         int next = 0, best = -1, kind = -1;
         float ms[kSolveVariants] = {};
@@ -537,18 +539,22 @@ void ensure_points(mgr_handle *h, int64_t npts) {
 
 constexpr int64_t kBytesPerPoint = sizeof(int32_t) + 2 * sizeof(double) + sizeof(MixedPoint);
 
+// 60% of the free device memory plus what the handle's point buffers hold.
 int64_t default_budget(mgr_handle *h) {
     size_t fr = 0, tot = 0;
     ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
-    return (int64_t)(0.6 * (double)fr);
+    return (int64_t)(0.6 * (double)fr) + h->tcap * kBytesPerPoint;
 }
 
 void do_trace(mgr_handle *h) {
     need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
     set_device(h);
-    free_traces(h);
-    h->tune[0] = mgr_handle::Tune{};   // the kernel choice depends on the trace
-    h->tune[1] = mgr_handle::Tune{};
+    // keep the point buffers of an earlier trace for reuse (freeing and
+    // allocating several GB costs more than the trace itself)
+    h->traced = false;
+    h->stored = false;
+    h->gen++;
+    const int old_max_pair = h->max_pair_points;
     const int64_t N = h->N, R = h->nrays, n = R * N;
     h->max_pair_points = 0;
     if (!h->len_all) h->len_all = dalloc<int32_t>(h, n, nullptr);
@@ -576,10 +582,14 @@ void do_trace(mgr_handle *h) {
         }
     }
     h->updates_per_solve = U * h->nfreqs;
+    if (h->max_pair_points != old_max_pair) {   // the kernel choice depends on it
+        h->tune[0] = mgr_handle::Tune{};
+        h->tune[1] = mgr_handle::Tune{};
+    }
     h->total_points = total;
     const int64_t budget = h->trace_budget > 0 ? h->trace_budget : default_budget(h);
     if (total * kBytesPerPoint <= budget) {
-        h->off_all = dalloc<int64_t>(h, n, nullptr);
+        if (!h->off_all) h->off_all = dalloc<int64_t>(h, n, nullptr);
         const int64_t tot = scan_lengths(h, h->len_all, h->off_all, n);
         ensure_points(h, tot);
         TraceView t{0, N, (int)R, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
@@ -677,12 +687,32 @@ void solve_prepare(mgr_handle *h, int precision) {
     }
 }
 
+// Tuning results shared by the handles of this process, keyed by device,
+// precision and the shape that decides the kernel's behaviour.
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune_cache;
+
+std::string tune_key(mgr_handle *h, int precision) {
+    return std::to_string(h->device) + "/" + std::to_string(precision) + "/" +
+           std::to_string(h->nfreqs) + "/" + std::to_string(h->nquads) + "/" +
+           std::to_string(h->nrad) + "/" + std::to_string(h->mv.overlap) + "/" +
+           std::to_string(h->max_pair_points / 32) + "/" + std::to_string(h->stored ? 1 : 0);
+}
+
 // The compiled variant for the next solve: a candidate still to be timed
 // while autotuning, else the fastest timed one, else the default (-1).
 int solve_variant(mgr_handle *h, int precision, bool *timing) {
     mgr_handle::Tune &tu = h->tune[precision == MGR_MIXED];
     *timing = false;
     if (tu.best >= 0) return tu.best;
+    if (h->autotune == 1) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(tune_key(h, precision));
+        if (it != g_tune_cache.end()) {
+            tu.best = it->second;
+            return tu.best;
+        }
+    }
     if (h->autotune && tu.next < kSolveVariants) {
         *timing = true;
         return tu.next;
@@ -699,6 +729,8 @@ void tune_record(mgr_handle *h, int precision, int variant, float ms) {
         for (int v = 1; v < kSolveVariants; v++)
             if (tu.ms[v] < tu.ms[best]) best = v;
         tu.best = best;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[tune_key(h, precision)] = best;
     }
 }
 
@@ -1215,7 +1247,8 @@ mgr_status mgr_get_segment_results(mgr_handle *h, double *stats, int64_t *iterat
 
 mgr_status mgr_set_autotune(mgr_handle *h, int32_t enable) {
     return run(h, [&] {
-        h->autotune = enable != 0;
+        need(enable >= 0 && enable <= 2, MGR_ERR_INVALID_ARG, "autotune mode is 0, 1 or 2");
+        h->autotune = enable;
         h->tune[0] = mgr_handle::Tune{};
         h->tune[1] = mgr_handle::Tune{};
     });

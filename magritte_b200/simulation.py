@@ -143,8 +143,10 @@ class Simulation:
         return st, it
 
     # ------------------------------------------------------------ tuning
-    def set_autotune(self, enable: bool = True):
-        self._ck(self._lib.mgr_set_autotune(self._h, int(bool(enable))))
+    def set_autotune(self, mode=True):
+        """True / 1: tune the solve kernel (reusing this process's results
+        for the same shape); 2: always re-time; False / 0: off."""
+        self._ck(self._lib.mgr_set_autotune(self._h, int(mode)))
 
     def tuning(self, precision="mixed") -> dict:
         t = _capi.Tuning()

@@ -86,7 +86,7 @@ def test_autotuner_candidates_agree(gpu, precision):
     sim.compute_spectral_discretisation()
     sim.compute_boundary_intensities()
     sim.compute_LTE_level_populations()
-    sim.set_autotune(True)
+    sim.set_autotune(2)
     outs = []
     for _ in range(4):
         sim.compute_radiation_field(precision, keep_J=True)
