@@ -49,10 +49,6 @@ constexpr int kWarpsPerBlock = 4;
 // generic kernel, 8 for the staged one (measured best on the 64^3 wind).
 constexpr int kVariantBlocks[kSolveVariants] = {6, 7, 8};
 constexpr int kDefaultGeneric = 1, kDefaultStaged = 2;
-#ifndef MGR_STAGED_MAX_POINTS
-#define MGR_STAGED_MAX_POINTS 768
-#endif
-constexpr int kStagedMaxCap = MGR_STAGED_MAX_POINTS;   // points per ray pair in the staged buffer
 
 // 1/x for normal x of either sign: hardware estimate refined by two Newton-Raphson
 // steps y <- y (2 - x y) (accurate to about one ulp).
@@ -618,35 +614,34 @@ __device__ __forceinline__ void staged_eval(const StagedPt *p, int eo, float q, 
     t = e.x * rg * rcp_approx(chi);
 }
 
-#ifndef MGR_STAGED_NEWTON
-#define MGR_STAGED_NEWTON 1
-#endif
-// 1/x of the staged elimination: hardware estimate and MGR_STAGED_NEWTON
-// Newton-Raphson refinements.  One refinement leaves an error far below the
-// float rounding of the optical depths (the mixed J and ALO agree with the
-// two-refinement build to the same 6e-8 against FP64 on the 64^3 wind).
-__device__ __forceinline__ double rcp_chain(double x) {
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-#pragma unroll
-    for (int i = 0; i < MGR_STAGED_NEWTON; i++) y = fma(y, fma(-x, y, 1.0), y);
-    return y;
+// 2^-e for the binary exponent e of b > 0 (a normal double), built from the
+// exponent field: multiplying by it brings b into [1, 2) exactly.
+__device__ __forceinline__ double pow2_recip_scale(double b) {
+    const int hi = __double2hiint(b);
+    return __hiloint2double(0x7fe00000 - (hi & 0x7ff00000), 0);
 }
 
-struct HalfChain {
+// Scaled Rybicki-Hummer state in projective form: F~ = a/b, S~ = c/b.  A
+// step then needs no division:
+//     Pb = P b,  a <- Q (Pb + a),  b <- Pb + 2a,  c <- Q (t Pb + c)
+// (from F~ <- w/(P + 2w), w = Q (P + F~), and S~ <- (t P + S~) Q/(P + 2w),
+// multiplied through by b).  Every term is non-negative for non-negative
+// opacities, so nothing cancels; a, b, c are rescaled by a power of two
+// every second step, which keeps them in range for any optical depth.
+struct ProjChain {
     float chi_a, t_a, dzh_a;   // current point
-    double dh_prev, F, S;      // scaled Rybicki-Hummer state
+    double dh_prev, a, b, c;
 
     __device__ __forceinline__ void start(float chi, float t, float dzh) {
         chi_a = chi; t_a = t; dzh_a = dzh;
     }
-    // boundary row of the far end
+    // boundary row of the far end: F~ = dh(dh+1)/(2dh(dh+1)+1),
+    // S~ = dh(t dh + I)/(2dh(dh+1)+1)
     __device__ __forceinline__ void first(float chi_b, float t_b, float dzh_b, double I) {
         const double dh = (double)((chi_a + chi_b) * dzh_a);
-        const double dh1 = dh + 1.0;
-        const double D = rcp_chain(fma(2.0 * dh, dh1, 1.0));
-        F = dh * dh1 * D;
-        S = dh * fma((double)t_a, dh, I) * D;
+        a = dh * (dh + 1.0);
+        b = fma(2.0, a, 1.0);
+        c = dh * fma((double)t_a, dh, I);
         dh_prev = dh;
         chi_a = chi_b; t_a = t_b; dzh_a = dzh_b;
     }
@@ -654,96 +649,149 @@ struct HalfChain {
         const double dh = (double)((chi_a + chi_b) * dzh_a);
         const double H = dh_prev + dh;
         const double P = H * dh_prev, Q = H * dh;
-        const double w = Q * (P + F);
-        const double D = rcp_chain(fma(2.0, w, P));
-        F = w * D;
-        S = fma((double)t_a, P, S) * (Q * D);
+        const double Pb = P * b;
+        a = Q * (Pb + a);
+        c = Q * fma((double)t_a, Pb, c);
+        b = fma(2.0, a, Pb);
         dh_prev = dh;
         chi_a = chi_b; t_a = t_b; dzh_a = dzh_b;
     }
+    __device__ __forceinline__ void renorm() {
+        const double sc = pow2_recip_scale(b);
+        a *= sc; b *= sc; c *= sc;
+    }
 };
 
-// u and L at the origin for the staged pair: front points at [0, nfr)
-// (far end at nfr-1), back points at [nfr, nfr+nbk).
-__device__ __forceinline__ void staged_sweep(const StagedPt *pts, int nfr, int nbk, int eo,
-                                             float q, float floor_hat, const BdyCtx &bc,
-                                             const BinCtx &b, float chi_o, float t_o,
-                                             const ModelView &m, int origin, DevFlags *flags,
-                                             double &u, double &L) {
-    HalfChain fr, bk;
-    float chi, t;
-    const StagedPt *pf = pts + (nfr - 1);
-    staged_eval(pf, eo, q, floor_hat, chi, t);
-    fr.start(chi, t, pf->dzh);
-    const double I0 = boundary_intensity(bc, (1.0 + (double)pf->delta) * b.nu_o, pf->cell, flags);
-    if (nfr >= 2) {
-        pf--;
-        staged_eval(pf, eo, q, floor_hat, chi, t);
-        fr.first(chi, t, pf->dzh, I0);
-    } else {
-        fr.first(chi_o, t_o, 0.0f, I0);
-    }
-    double In = 0.0;
-    const StagedPt *pb = pts + (nfr + nbk - 1);
-    if (nbk > 0) {
-        staged_eval(pb, eo, q, floor_hat, chi, t);
-        bk.start(chi, t, pb->dzh);
-        In = boundary_intensity(bc, (1.0 + (double)pb->delta) * b.nu_o, pb->cell, flags);
-        if (nbk >= 2) {
-            pb--;
-            staged_eval(pb, eo, q, floor_hat, chi, t);
-            bk.first(chi, t, pb->dzh, In);
-        } else {
-            bk.first(chi_o, t_o, 0.0f, In);
+// Steps of the sweep held in shared memory at a time (per half).
+#ifndef MGR_STAGE_STEPS
+#define MGR_STAGE_STEPS 64
+#endif
+constexpr int kStageSteps = MGR_STAGE_STEPS;
+
+// u and L at the origin for one (pair, bin): the warp stages the two halves
+// window by window (kStageSteps steps of each), step s of the front being
+// its point nfr-1-s (the far end first) and likewise for the back; each
+// lane eliminates both halves toward the origin, in lock step while both
+// have points.
+__device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, const float2 *ek,
+                                            int K, int k0, int k1, int64_t ofr, int nfr,
+                                            int64_t obk, int nbk, int eo, float q, float floor_hat,
+                                            const BdyCtx &bc, const BinCtx &b, float chi_o, float t_o,
+                                            const ModelView &m, int origin, int lane,
+                                            DevFlags *flags, double &u, double &L) {
+    constexpr float kSqrtLog2e = 1.2011224087864498f;
+    ProjChain fr, bk;
+    double I0 = 0.0, In = 0.0;
+    float chi, t_, chi2, t2;
+    for (int s0 = 0; s0 < nfr; s0 += kStageSteps) {
+        const int s1 = min(s0 + kStageSteps, nfr);
+        const int nF = s1 - s0;
+        const int nB = max(0, min(s1, nbk) - s0);
+        for (int j = lane; j < nF + nB; j += 32) {
+            const bool front = j < nF;
+            const int st = s0 + (front ? j : j - nF);
+            const int64_t gi = front ? ofr + (nfr - 1 - st) : obk + (nbk - 1 - st);
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(t.mp) + gi);
+            const unsigned cell = (unsigned)__float_as_int(v.x);
+            float2 e0 = __ldg(ek + cell * K + k0);
+            float2 e1 = __ldg(ek + cell * K + k1);
+            if (e0.y < 0.0f) e0.x = __int_as_float(0x7fc00000);
+            if (e1.y < 0.0f) e1.x = __int_as_float(0x7fc00000);
+            float4 *dst = reinterpret_cast<float4 *>(buf + (front ? j : kStageSteps + (j - nF)));
+            dst[0] = make_float4(v.y, 0.5f * v.z, v.w * kSqrtLog2e, v.x);
+            dst[1] = make_float4(e0.x, e0.y, e1.x, e1.y);
         }
-    } else {
+        __syncwarp();
+        const StagedPt *F = buf - s0;                 // front step s at F[s]
+        const StagedPt *B = buf + kStageSteps - s0;   // back step s at B[s]
+        int s = s0;
+        if (s == 0) {
+            staged_eval(F, eo, q, floor_hat, chi, t_);
+            fr.start(chi, t_, F->dzh);
+            I0 = boundary_intensity(bc, (1.0 + (double)F->delta) * b.nu_o, F->cell, flags);
+            if (nbk > 0) {
+                staged_eval(B, eo, q, floor_hat, chi, t_);
+                bk.start(chi, t_, B->dzh);
+                In = boundary_intensity(bc, (1.0 + (double)B->delta) * b.nu_o, B->cell, flags);
+            }
+            s = 1;
+        }
+        if (s == 1 && s < s1) {
+            staged_eval(F + 1, eo, q, floor_hat, chi, t_);
+            fr.first(chi, t_, F[1].dzh, I0);
+            if (nbk > 1) {
+                staged_eval(B + 1, eo, q, floor_hat, chi, t_);
+                bk.first(chi, t_, B[1].dzh, In);
+            }
+            s = 2;
+        }
+        // both halves
+        const int e1 = min(s1, nbk);
+        for (; s + 1 < e1; s += 2) {
+            staged_eval(F + s, eo, q, floor_hat, chi, t_);
+            staged_eval(B + s, eo, q, floor_hat, chi2, t2);
+            fr.step(chi, t_, F[s].dzh);
+            bk.step(chi2, t2, B[s].dzh);
+            staged_eval(F + s + 1, eo, q, floor_hat, chi, t_);
+            staged_eval(B + s + 1, eo, q, floor_hat, chi2, t2);
+            fr.step(chi, t_, F[s + 1].dzh);
+            bk.step(chi2, t2, B[s + 1].dzh);
+            fr.renorm();
+            bk.renorm();
+        }
+        if (s < e1) {
+            staged_eval(F + s, eo, q, floor_hat, chi, t_);
+            staged_eval(B + s, eo, q, floor_hat, chi2, t2);
+            fr.step(chi, t_, F[s].dzh);
+            bk.step(chi2, t2, B[s].dzh);
+            fr.renorm();
+            bk.renorm();
+            s++;
+        }
+        // the rest of the front half
+        for (; s + 1 < s1; s += 2) {
+            staged_eval(F + s, eo, q, floor_hat, chi, t_);
+            fr.step(chi, t_, F[s].dzh);
+            staged_eval(F + s + 1, eo, q, floor_hat, chi, t_);
+            fr.step(chi, t_, F[s + 1].dzh);
+            fr.renorm();
+        }
+        if (s < s1) {
+            staged_eval(F + s, eo, q, floor_hat, chi, t_);
+            fr.step(chi, t_, F[s].dzh);
+            fr.renorm();
+        }
+        __syncwarp();
+    }
+    // the origin row
+    if (nfr == 1) fr.first(chi_o, t_o, 0.0f, I0);
+    else fr.step(chi_o, t_o, 0.0f);
+    const double to = (double)t_o;
+    if (nbk == 0) {
         const int bo = __ldg(m.cell2bdy + origin);
         if (bo >= 0) In = __ldg(m.ibdy + (int64_t)bo * m.nfreqs + b.f);
         else atomicAdd(&flags->trace_err, 1ull);
-    }
-    // both halves have interior points: advance them in lock step
-    if (nbk >= 2) {
-        const int nlock = nbk - 2;
-#pragma unroll 2
-        for (int i = 0; i < nlock; i++) {
-            pf--; pb--;
-            float chi_p, t_p, chi_q, t_q;
-            staged_eval(pf, eo, q, floor_hat, chi_p, t_p);
-            staged_eval(pb, eo, q, floor_hat, chi_q, t_q);
-            fr.step(chi_p, t_p, pf->dzh);
-            bk.step(chi_q, t_q, pb->dzh);
-        }
-        bk.step(chi_o, t_o, 0.0f);
-    }
-    // the rest of the front half
-    const int nrest = (int)(pf - pts);
-#pragma unroll 2
-    for (int i = 0; i < nrest; i++) {
-        pf--;
-        staged_eval(pf, eo, q, floor_hat, chi, t);
-        fr.step(chi, t, pf->dzh);
-    }
-    if (nfr >= 2) fr.step(chi_o, t_o, 0.0f);
-
-    const double to = (double)t_o;
-    if (nbk == 0) {
+        // u = (dh (t dh + In) + S~)/(dh (dh + 1) + F~), times b
         const double dh = fr.dh_prev;
-        const double D = rcp_chain(fma(dh, dh + 1.0, fr.F));
-        u = fma(dh, fma(to, dh, In), fr.S) * D;
-        L = dh * dh * D;
+        const double D = rcp_pos(fma(dh * (dh + 1.0), fr.b, fr.a));
+        u = fma(dh * fma(to, dh, In), fr.b, fr.c) * D;
+        L = dh * dh * fr.b * D;
         return;
     }
+    if (nbk == 1) bk.first(chi_o, t_o, 0.0f, In);
+    else bk.step(chi_o, t_o, 0.0f);
+    // u = (t PQ + S~f Q + S~b P)/(F~f Q + F~b P + PQ), times bf bb
     const double H = fr.dh_prev + bk.dh_prev;
     const double P = H * fr.dh_prev, Q = H * bk.dh_prev;
-    const double PQ = P * Q;
-    const double D = rcp_chain(fma(fr.F, Q, fma(bk.F, P, PQ)));
-    u = fma(to, PQ, fma(fr.S, Q, bk.S * P)) * D;
-    L = PQ * D;
+    const double PQB = P * Q * (fr.b * bk.b);
+    const double D = rcp_pos(fma(fr.a * bk.b, Q, fma(bk.a * fr.b, P, PQB)));
+    u = fma(to, PQB, fma(fr.c * bk.b, Q, bk.c * fr.b * P)) * D;
+    L = PQB * D;
 }
 
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
-    formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, int cap, DevFlags *flags) {
+    formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
@@ -751,6 +799,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     const int o = (int)(t.o_begin + oi);
     if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
+    constexpr int cap = 2 * kStageSteps;
     StagedPt *pts = reinterpret_cast<StagedPt *>(smem_raw) + (size_t)warp * cap;
     double *sJ = reinterpret_cast<double *>(reinterpret_cast<StagedPt *>(smem_raw) +
                                             (size_t)kWarpsPerBlock * cap) + (size_t)warp * 2 * K;
@@ -760,8 +809,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     const float2 *ek = a.ehat_khat;
     const BdyCtx bc = bdy_ctx(m);
     const float floor_hat = (float)(1.0E-26 * a.mixed_scale);
-    const float kSqrtLog2e = 1.2011224087864498f;
-
     const double pw_o = m.pw[o];
     const int nchunks = (nf + 31) >> 5;
     for (int c = 0; c < nchunks; c++) {
@@ -812,23 +859,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
                 Jf += 2.0 * wr * (0.5 * (I + I));
                 continue;
             }
-            const int np = nfr + nbk;
-            for (int j = lane; j < np; j += 32) {
-                const int64_t gi = j < nfr ? ofr + j : obk + (j - nfr);
-                const float4 v = __ldg(reinterpret_cast<const float4 *>(t.mp) + gi);
-                const unsigned cell = (unsigned)__float_as_int(v.x);
-                float2 e0 = __ldg(ek + cell * K + k0);
-                float2 e1 = __ldg(ek + cell * K + k1);
-                if (e0.y < 0.0f) e0.x = __int_as_float(0x7fc00000);
-                if (e1.y < 0.0f) e1.x = __int_as_float(0x7fc00000);
-                float4 *dst = reinterpret_cast<float4 *>(pts + j);
-                dst[0] = make_float4(v.y, 0.5f * v.z, v.w * kSqrtLog2e, v.x);
-                dst[1] = make_float4(e0.x, e0.y, e1.x, e1.y);
-            }
-            __syncwarp();
             double u, L;
-            staged_sweep(pts, nfr, nbk, eo, b.q, floor_hat, bc, b, chi_o, t_o, m, o, flags, u, L);
-            __syncwarp();
+            staged_pair(pts, t, ek, K, k0, k1, ofr, nfr, obk, nbk, eo, b.q, floor_hat, bc, b, chi_o,
+                        t_o, m, o, lane, flags, u, L);
             if (!(isfinite(u) && isfinite(L))) {
                 const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
                 if (slot < (unsigned long long)a.patch_cap) a.patch[slot] = make_int4(o, r, fc, 0);
@@ -868,8 +901,7 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
     if (t.o_count == 0) return cudaSuccess;
     const int64_t blocks = (t.o_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const size_t shmem = (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
-    const bool staged = precision == MGR_MIXED && !m.overlap && m.nquads >= 31 &&
-                        a.max_pair_points > 0 && a.max_pair_points <= kStagedMaxCap;
+    const bool staged = precision == MGR_MIXED && !m.overlap && m.nquads >= 31;
     if (kind) *kind = staged ? 1 : 0;
     if (variant < 0 || variant >= kSolveVariants) variant = staged ? kDefaultStaged : kDefaultGeneric;
     auto run = [&](auto pol) {
@@ -901,14 +933,13 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         run(pol);
     };
     if (staged) {
-        const int cap = (int)((a.max_pair_points + 1) & ~1);
-        const size_t sm = (size_t)kWarpsPerBlock * cap * sizeof(StagedPt) +
+        const size_t sm = (size_t)kWarpsPerBlock * 2 * kStageSteps * sizeof(StagedPt) +
                           (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
         auto go = [&](auto kern) -> cudaError_t {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)sm);
             if (e != cudaSuccess) return e;
-            kern<<<(unsigned)blocks, kWarpsPerBlock * 32, sm, s>>>(m, t, a, cap, flags);
+            kern<<<(unsigned)blocks, kWarpsPerBlock * 32, sm, s>>>(m, t, a, flags);
             return cudaSuccess;
         };
         cudaError_t e;
