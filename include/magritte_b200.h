@@ -224,6 +224,13 @@ mgr_status mgr_get_frequencies(mgr_handle *h, double *nu);            /* [ncells
  * stream) and the ray-point-frequency updates it did. */
 mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates);
 
+/* Mixed precision: (origin, pair, bin) solves of the last formal solve that
+ * were redone in double (inverted lines driving the opacity below half its
+ * 1e-26 floor, or a float failure), and the number of mixed solves since
+ * mgr_create that were redone entirely in double because that list
+ * overflowed.  No reference counterpart (the reference solves in double). */
+mgr_status mgr_get_patch_stats(mgr_handle *h, int64_t *patched, int64_t *fallbacks);
+
 /* Synchronises the handle's stream. */
 mgr_status mgr_synchronize(mgr_handle *h);
 

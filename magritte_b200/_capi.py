@@ -38,6 +38,7 @@ EXPORTS = (
     "mgr_convergence_noalloc", "mgr_mlp_param_count", "mgr_get_features", "mgr_get_lte_logfrac",
     "mgr_warm_start", "mgr_mlp_train", "mgr_mlp_forward", "mgr_mlp_loss_grad",
     "mgr_set_segments", "mgr_get_segment_results", "mgr_set_autotune", "mgr_get_tuning",
+    "mgr_get_patch_stats",
 )
 MLP_FEATURES = 10
 MLP_HIDDEN = 128
@@ -145,6 +146,7 @@ def load(build_if_missing: bool = True):
     L.mgr_mlp_forward.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _i64, _P]
     L.mgr_mlp_loss_grad.argtypes = [C.c_int, C.POINTER(MlpDesc), _P, _P, _P, _i64, _P, _P]
     L.mgr_set_segments.argtypes = [_P, _i64, _P]
+    L.mgr_get_patch_stats.argtypes = [_P, C.POINTER(_i64), C.POINTER(_i64)]
     L.mgr_get_segment_results.argtypes = [_P, _P, _P]
     L.mgr_set_autotune.argtypes = [_P, _i32]
     L.mgr_get_tuning.argtypes = [_P, _i32, C.POINTER(Tuning)]

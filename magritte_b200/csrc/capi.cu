@@ -101,6 +101,7 @@ struct mgr_handle {
     unsigned long long *h_patch = nullptr;   // pinned copy of patch_count
     int64_t patch_cap = 0;
     int64_t last_patched = 0;
+    int64_t fp64_fallbacks = 0;        // mixed solves redone in double (patch list full)
 
     // batch of independent models (nseg > 0)
     int64_t nseg = 0;
@@ -680,7 +681,9 @@ void solve_prepare(mgr_handle *h, int precision) {
     if (!h->bdy_set) boundary_table(h);
     if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
     if (precision == MGR_MIXED && !h->patch) {
-        h->patch_cap = 1 << 20;
+        // room for 1 in 1000 (origin, pair, bin) solves, 1M..64M entries
+        const double all = (double)h->N * h->npairs * h->nfreqs;
+        h->patch_cap = (int64_t)std::min(std::max(all / 1000.0, (double)(1 << 20)), (double)(1 << 26));
         h->patch = dalloc<int4>(h, h->patch_cap, nullptr);
         h->patch_count = dalloc<unsigned long long>(h, 1, nullptr);
         h->gen++;
@@ -782,6 +785,7 @@ int graph_run(mgr_handle *h, mgr_handle::Graph &g, int key, const std::function<
 void finish_solve(mgr_handle *h, int precision, int variant, bool timing, int64_t patched) {
     if (precision == MGR_MIXED && h->h_flags->patch_overflow) {
         // more float failures than the patch list holds: solve in double
+        h->fp64_fallbacks++;
         do_solve(h, MGR_FP64, false);
         return;
     }
@@ -1321,6 +1325,13 @@ mgr_status mgr_get_frequencies(mgr_handle *h, double *nu) {
                     nu[(p * h->nrad + k) * h->nquads + z] = line[k] + a;
                 }
             }
+    });
+}
+
+mgr_status mgr_get_patch_stats(mgr_handle *h, int64_t *patched, int64_t *fallbacks) {
+    return run(h, [&] {
+        if (patched) *patched = h->last_patched;
+        if (fallbacks) *fallbacks = h->fp64_fallbacks;
     });
 }
 

@@ -264,10 +264,12 @@ struct MixedPolicy {
             chi += (float)(ca * m.mixed_scale);
         }
         // Negative line opacity (population inversion, which the
-        // reference's iteration allows) cancels badly in float near zero:
-        // such a point poisons its pair with a NaN source function, and the
-        // pair is solved again in double by the patch pass.
-        if (chi < floor_hat) eta = __int_as_float(0x7fc00000);
+        // reference's iteration allows) that takes chi below half the floor
+        // cancels badly in float: such a point poisons its pair with a NaN
+        // source function, and the pair is solved again in double by the
+        // patch pass.  Above half the floor the float sum loses at most a
+        // factor two of relative precision.
+        if (chi < 0.5f * floor_hat) eta = __int_as_float(0x7fc00000);
         t = __fdividef(eta, chi);
     }
     __device__ __forceinline__ static double dtau(float chi_a, float chi_b, float dzs) {
@@ -409,11 +411,8 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
 // sweep produced a non-finite u or L (near-zero or negative opacities from
 // transient population inversion, where float runs out of range) are
 // solved again in double, one thread per entry, and added to the outputs.
-__global__ void patch_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t n = min((unsigned long long)*a.patch_count, (unsigned long long)a.patch_cap);
-    if (i >= n) return;
-    const int4 e = a.patch[i];
+__device__ __noinline__ void patch_entry(const ModelView &m, const TraceView &t, const SolveArgs &a,
+                                         DevFlags *flags, int4 e) {
     const int o = e.x, r = e.y, f = e.z;
     const int64_t oi = o - t.o_begin;
     const int nq = m.nquads, nf = m.nfreqs, K = m.nrad;
@@ -452,6 +451,13 @@ __global__ void patch_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *fl
     atomicAdd(a.Jlin + (int64_t)o * K + b.k, m.qw[z] * (2.0 * wr * u));
     atomicAdd(a.Lam + (int64_t)o * K + b.k, lam_pre * wr * L);
     if (a.J) atomicAdd(a.J + (int64_t)o * nf + f, 2.0 * wr * u);
+}
+
+__global__ void patch_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
+    const int64_t n = min((unsigned long long)*a.patch_count, (unsigned long long)a.patch_cap);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        patch_entry(m, t, a, flags, a.patch[i]);
 }
 
 template <class Pol, int kMinBlocks>
@@ -577,8 +583,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
 
 // One traced point of the staged pair: the float record and the opacity
 // pairs (eps, kap) * INVSQRTPI / pw * X of the chunk's two lines.  A point
-// whose line opacity is negative carries a NaN emissivity, which sends the
-// (pair, bin) to the double-precision patch pass.
+// whose negative line opacity can take chi below half the 1e-26 floor
+// carries a NaN emissivity, which sends the (pair, bin) to the
+// double-precision patch pass.
 struct __align__(16) StagedPt {
     float delta;   // Doppler shift - 1
     float dzh;     // dZ / (4 X): dh = (chi_a + chi_b) * dzh for chi scaled by X
@@ -680,6 +687,9 @@ __device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, c
                                             const ModelView &m, int origin, int lane,
                                             DevFlags *flags, double &u, double &L) {
     constexpr float kSqrtLog2e = 1.2011224087864498f;
+    // an inverted line whose opacity can take chi below half the floor
+    // (the profile factor (1 + off) exp(-x^2) stays below 1.001)
+    const float neg_cut = -0.499f * floor_hat;
     ProjChain fr, bk;
     double I0 = 0.0, In = 0.0;
     float chi, t_, chi2, t2;
@@ -695,8 +705,8 @@ __device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, c
             const unsigned cell = (unsigned)__float_as_int(v.x);
             float2 e0 = __ldg(ek + cell * K + k0);
             float2 e1 = __ldg(ek + cell * K + k1);
-            if (e0.y < 0.0f) e0.x = __int_as_float(0x7fc00000);
-            if (e1.y < 0.0f) e1.x = __int_as_float(0x7fc00000);
+            if (e0.y < neg_cut) e0.x = __int_as_float(0x7fc00000);
+            if (e1.y < neg_cut) e1.x = __int_as_float(0x7fc00000);
             float4 *dst = reinterpret_cast<float4 *>(buf + (front ? j : kStageSteps + (j - nF)));
             dst[0] = make_float4(v.y, 0.5f * v.z, v.w * kSqrtLog2e, v.x);
             dst[1] = make_float4(e0.x, e0.y, e1.x, e1.y);
@@ -828,11 +838,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
         const int k1 = min(K - 1, k0 + 1);
         const int eo = b.k != k0 ? 3 : 2;   // float2 index of this lane's line in a StagedPt
 
-        // origin in double; a negative line opacity there poisons the bin
+        // origin in double; an inverted line taking chi below half the floor
+        // there poisons the bin
         double e64, c64;
         eta_chi_double(m, a.eps, a.kap, o, b.nu_o, b.k, b.k, e64, c64);
         const float chi_o = (float)(c64 * m.mixed_scale);
-        const float t_o = c64 < 1.0E-26 ? __int_as_float(0x7fc00000) : (float)(e64 / c64);
+        const float t_o = c64 < 0.5E-26 ? __int_as_float(0x7fc00000) : (float)(e64 / c64);
         const double width_o = line_k * pw_o;
         const double iw = 1.0 / width_o;
         const double xo = iw * (b.nu_o - line_k);
@@ -958,7 +969,7 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         if (e != cudaSuccess) return e;
         // entries beyond patch_cap are counted in DevFlags; the host then
         // solves again in double
-        const unsigned pblocks = (unsigned)((a.patch_cap + 127) / 128);
+        const unsigned pblocks = (unsigned)std::min<int64_t>((a.patch_cap + 127) / 128, 148 * 16);
         patch_kernel<<<pblocks, 128, 0, s>>>(m, t, a, flags);
     } else {
         if (m.overlap) fp64(Fp64Policy<true>{});

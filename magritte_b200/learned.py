@@ -11,6 +11,8 @@ forward, backward and Adam kernels (``mgr_mlp_train``).
 
     python -m magritte_b200.learned train --n 32 --models 12 --epochs 600 \
         --out magritte_b200/weights/wind_rotor10.npz
+    python -m magritte_b200.learned train --family turb --n 64 --models 8 --nlev 21 \
+        --epochs 300 --subsample 0.25 --out magritte_b200/weights/turb_rotor21.npz
 """
 from __future__ import annotations
 
@@ -142,10 +144,11 @@ def converged_samples(model, precision="mixed", tol=1e-6, max_iter=400, device=0
     the iteration count."""
     from .simulation import Simulation
     sim = Simulation(model, device=device)
+    sim.set_autotune(True)
     sim.compute_spectral_discretisation()
     sim.compute_boundary_intensities()
     sim.compute_LTE_level_populations()
-    it = sim.compute_level_populations(True, max_iter, precision, tol_max_rel=tol)
+    it = sim.compute_level_populations(True, max_iter, precision, tol_max_rel=tol, use_graph=True)
     X, L, T = samples_from(sim, sim.population)
     sim.close()
     return X, L, T, it
@@ -165,9 +168,26 @@ def wind_family(n: int, count: int, seed0: int, nlev: int = 10, nside: int = 2):
     return out
 
 
+def turb_family(n: int, count: int, seed0: int, nlev: int = 21):
+    """Seeded members of the turbulent-cloud family (lognormal density,
+    k^-4 velocity field): mean density and velocity dispersion drawn around
+    the 128^3 cloud's 1e11 m^-3 and 2 km/s, new random fields per seed."""
+    out = []
+    for i in range(count):
+        rng = np.random.default_rng(seed0 + i)
+        out.append(M.turbulent_cloud(n, seed=seed0 + i, nlev=nlev, npairs=48, nquads=41,
+                                     mean_h2=10 ** rng.uniform(10.6, 11.4),
+                                     vrms=rng.uniform(1.5e3, 2.5e3),
+                                     name=f"turb{n}_s{seed0 + i}"))
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("--family", choices=["wind", "turb"], default="wind")
+    ap.add_argument("--subsample", type=float, default=1.0,
+                    help="fraction of each model's cells used for training")
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--models", type=int, default=12)
     ap.add_argument("--seed0", type=int, default=100)
@@ -178,16 +198,22 @@ def main(argv=None):
     a = ap.parse_args(argv)
     t0 = time.time()
     Xs, Ls, Ts, its = [], [], [], []
-    for m in wind_family(a.n, a.models, a.seed0, a.nlev):
+    fam = wind_family if a.family == "wind" else turb_family
+    rng = np.random.default_rng(a.seed0)
+    for m in fam(a.n, a.models, a.seed0, a.nlev):
+        t_m = time.time()
         X, L, T, it = converged_samples(m)
+        if a.subsample < 1.0:
+            keep = rng.random(X.shape[0]) < a.subsample
+            X, L, T = X[keep], L[keep], T[keep]
         Xs.append(X); Ls.append(L); Ts.append(T); its.append(it)
-        print(f"{m.name}: {it} iterations", flush=True)
+        print(f"{m.name}: {it} iterations, {time.time() - t_m:.1f} s", flush=True)
     X, L, T = np.concatenate(Xs), np.concatenate(Ls), np.concatenate(Ts)
     t1 = time.time()
     net = WarmStartNet(a.nlev).init(0)
     hist = net.train(X, L, T, epochs=a.epochs)
     t2 = time.time()
-    net.meta = dict(family="wind", n=a.n, models=a.models, seed0=a.seed0, nlev=a.nlev,
+    net.meta = dict(family=a.family, n=a.n, subsample=a.subsample, models=a.models, seed0=a.seed0, nlev=a.nlev,
                     epochs=a.epochs, samples=int(X.shape[0]), final_loss=float(hist[-1]),
                     first_loss=float(hist[0]), ali_iterations=its,
                     data_s=round(t1 - t0, 1), train_s=round(t2 - t1, 1))

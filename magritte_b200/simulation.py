@@ -142,6 +142,13 @@ class Simulation:
         self._ck(self._lib.mgr_get_segment_results(self._h, _capi.ptr(st), _capi.ptr(it)))
         return st, it
 
+    def patch_stats(self):
+        """(solves of the last mixed formal solve redone in double, mixed
+        solves redone entirely in double so far)."""
+        a, b = C.c_int64(0), C.c_int64(0)
+        self._ck(self._lib.mgr_get_patch_stats(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
     # ------------------------------------------------------------ tuning
     def set_autotune(self, mode=True):
         """True / 1: tune the solve kernel (reusing this process's results
