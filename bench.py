@@ -110,6 +110,17 @@ def workload_config(name, model, prec, start="LTE"):
     return cfg
 
 
+def max_over_ranks(values):
+    """Element-wise max of `values` over the ranks of the default process
+    group (NCCL: through a device tensor; gloo: on the host)."""
+    import torch
+    import torch.distributed as tdist
+    dev = "cuda" if tdist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(list(values), dtype=torch.float64, device=dev)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -379,9 +390,7 @@ def run_b200(args):
 
     # ---- multi-GPU: max over ranks
     if dist:
-        t = torch.tensor([t_step, statistics.mean(e2e)], dtype=torch.float64, device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        t_step, e2e_t = float(t[0]), float(t[1])
+        t_step, e2e_t = max_over_ranks([t_step, statistics.mean(e2e)])
         tdist.barrier()
         tdist.destroy_process_group()
     else:
