@@ -681,9 +681,9 @@ void solve_prepare(mgr_handle *h, int precision) {
     if (!h->bdy_set) boundary_table(h);
     if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
     if (precision == MGR_MIXED && !h->patch) {
-        // room for 1 in 1000 (origin, pair, bin) solves, 1M..64M entries
+        // room for 1 in 100 (origin, pair, bin) solves, 1M..64M entries
         const double all = (double)h->N * h->npairs * h->nfreqs;
-        h->patch_cap = (int64_t)std::min(std::max(all / 1000.0, (double)(1 << 20)), (double)(1 << 26));
+        h->patch_cap = (int64_t)std::min(std::max(all / 100.0, (double)(1 << 20)), (double)(1 << 26));
         h->patch = dalloc<int4>(h, h->patch_cap, nullptr);
         h->patch_count = dalloc<unsigned long long>(h, 1, nullptr);
         h->gen++;

@@ -290,34 +290,55 @@ struct MixedPolicy {
 
 // ------------------------------------------------------------------ chains
 
-// Elimination of one half of the ray pair from its far end toward the origin.
+// 2^-e for the binary exponent e of b > 0 (a normal double), built from the
+// exponent field: multiplying by it brings b into [1, 2) exactly.
+__device__ __forceinline__ double pow2_recip_scale(double b) {
+    const int hi = __double2hiint(b);
+    return __hiloint2double(0x7fe00000 - (hi & 0x7ff00000), 0);
+}
+
+// Elimination of one half of the ray pair from its far end toward the
+// origin, on half optical depths dh = dtau/2 in projective form: the scaled
+// Rybicki-Hummer quantities are F~ = a/b and S~ = c/b (F~ = F'/2, S~ = S/2
+// for the reference's F' = F/(1+F) and S), and one step toward the origin is
+//     H = dh_far + dh_near, P = H dh_far, Q = H dh_near, Pb = P b,
+//     a <- Q (Pb + a),  c <- Q (t Pb + c),  b <- Pb + 2a
+// which is F~ <- w/(P + 2w), S~ <- (t P + S~) Q/(P + 2w) with
+// w = Q (P + F~), multiplied through by b: no division per point.  For
+// non-negative opacities every term is non-negative.  a, b, c are brought
+// back to b in [1, 2) by a power of two after each step.
 template <class Pol>
 struct Chain {
     using Real = typename Pol::Real;
     Real chi_a, t_a;      // current point
     Real dz_a;            // its increment toward the origin (policy units)
-    double F, S, dtau_prev;
+    double dh_prev, a, b, c;
 
-    // row of the far end (boundary row: B = 1 + 2/dtau + 2/dtau^2,
-    // S = t + 2 I/dtau)
+    // boundary row of the far end: F~ = dh(dh+1)/(2dh(dh+1)+1),
+    // S~ = dh(t dh + I)/(2dh(dh+1)+1)
     __device__ __forceinline__ void first(Real chi_b, Real t_b, Real dz_b, double I) {
-        const double d = Pol::dtau(chi_a, chi_b, dz_a);
-        const double D = rcp_pos(fma(d, d + 2.0, 2.0));
-        F = d * (d + 2.0) * D;
-        S = fma((double)t_a * d, d, 2.0 * I * d) * D;
-        dtau_prev = d;
+        const double dh = 0.5 * Pol::dtau(chi_a, chi_b, dz_a);
+        a = dh * (dh + 1.0);
+        b = fma(2.0, a, 1.0);
+        c = dh * fma((double)t_a, dh, I);
+        dh_prev = dh;
         chi_a = chi_b;
         t_a = t_b;
         dz_a = dz_b;
     }
     __device__ __forceinline__ void step(Real chi_b, Real t_b, Real dz_b) {
-        const double d = Pol::dtau(chi_a, chi_b, dz_a);
-        const double h = 0.5 * (dtau_prev + d);
-        const double p = h * dtau_prev, q = h * d;
-        const double D = rcp_pos(fma(p, 1.0 + q, q * F));
-        S = fma((double)t_a, p, S) * D * q;
-        F = q * (p + F) * D;
-        dtau_prev = d;
+        const double dh = 0.5 * Pol::dtau(chi_a, chi_b, dz_a);
+        const double H = dh_prev + dh;
+        const double P = H * dh_prev, Q = H * dh;
+        const double Pb = P * b;
+        a = Q * (Pb + a);
+        c = Q * fma((double)t_a, Pb, c);
+        b = fma(2.0, a, Pb);
+        const double sc = pow2_recip_scale(b);
+        a *= sc;
+        b *= sc;
+        c *= sc;
+        dh_prev = dh;
         chi_a = chi_b;
         t_a = t_b;
         dz_a = dz_b;
@@ -391,20 +412,20 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
 
     const double to = (double)t_o;
     if (nbk == 0) {
-        // the origin is the last row: S_d = t + 2 I_n / dtau
-        const double d = fr.dtau_prev;
-        const double den = rcp_pos(fma(d, d + 2.0, 2.0 * fr.F));
-        u = fma(to * d, d, fma(2.0 * In, d, 2.0 * fr.S)) * den;
-        L = d * d * den;
+        // the origin is the last row: u = (dh (t dh + In) + S~)/(dh (dh + 1) + F~)
+        const double dh = fr.dh_prev;
+        const double D = rcp_pos(fma(dh * (dh + 1.0), fr.b, fr.a));
+        u = fma(dh * fma(to, dh, In), fr.b, fr.c) * D;
+        L = dh * dh * fr.b * D;
         return;
     }
-    // origin row: A_o from the front step, C_o from the back step
-    const double h = 0.5 * (fr.dtau_prev + bk.dtau_prev);
-    const double iA = h * fr.dtau_prev, iC = h * bk.dtau_prev;
-    const double iAC = iA * iC;
-    const double den = rcp_pos(fma(fr.F, iC, fma(bk.F, iA, iAC)));
-    u = fma(to, iAC, fma(fr.S, iC, bk.S * iA)) * den;
-    L = iAC * den;
+    // origin row: u = (t PQ + S~f Q + S~b P)/(F~f Q + F~b P + PQ), times bf bb
+    const double H = fr.dh_prev + bk.dh_prev;
+    const double P = H * fr.dh_prev, Q = H * bk.dh_prev;
+    const double PQB = P * Q * (fr.b * bk.b);
+    const double D = rcp_pos(fma(fr.a * bk.b, Q, fma(bk.a * fr.b, P, PQB)));
+    u = fma(to, PQB, fma(fr.c * bk.b, Q, bk.c * fr.b * P)) * D;
+    L = PQB * D;
 }
 
 // Patch pass of the mixed solve: (origin, pair, bin) entries whose float
@@ -582,10 +603,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
 // L = PQ/(...) with P, Q built from the two segments at the origin.
 
 // One traced point of the staged pair: the float record and the opacity
-// pairs (eps, kap) * INVSQRTPI / pw * X of the chunk's two lines.  A point
-// whose negative line opacity can take chi below half the 1e-26 floor
-// carries a NaN emissivity, which sends the (pair, bin) to the
-// double-precision patch pass.
+// pairs (eps, kap) * INVSQRTPI / pw * X of the chunk's two lines.
 struct __align__(16) StagedPt {
     float delta;   // Doppler shift - 1
     float dzh;     // dZ / (4 X): dh = (chi_a + chi_b) * dzh for chi scaled by X
@@ -609,6 +627,9 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // bin sits q = pw_o * root widths from its line: with off = nu/line - 1,
 // chi X = 1e-26 X + Khat (1 + off) 2^-(off ipws)^2, the profile vanishing
 // (flushed to zero) beyond ~9.3 widths, inside the reference's 11-width cut.
+// kCheck (windows holding a strongly inverted line): a chi below half the
+// floor at this bin poisons the pair with a NaN source function.
+template <bool kCheck>
 __device__ __forceinline__ void staged_eval(const StagedPt *p, int eo, float q, float floor_hat,
                                             float &chi, float &t) {
     const float4 r = *reinterpret_cast<const float4 *>(p);
@@ -619,14 +640,9 @@ __device__ __forceinline__ void staged_eval(const StagedPt *p, int eo, float q, 
     const float rg = fmaf(off, g, g);
     chi = fmaf(e.y, rg, floor_hat);
     t = e.x * rg * rcp_approx(chi);
+    if (kCheck && chi < 0.5f * floor_hat) t = __int_as_float(0x7fc00000);
 }
 
-// 2^-e for the binary exponent e of b > 0 (a normal double), built from the
-// exponent field: multiplying by it brings b into [1, 2) exactly.
-__device__ __forceinline__ double pow2_recip_scale(double b) {
-    const int hi = __double2hiint(b);
-    return __hiloint2double(0x7fe00000 - (hi & 0x7ff00000), 0);
-}
 
 // Scaled Rybicki-Hummer state in projective form: F~ = a/b, S~ = c/b.  A
 // step then needs no division:
@@ -675,11 +691,80 @@ struct ProjChain {
 #endif
 constexpr int kStageSteps = MGR_STAGE_STEPS;
 
+// The sweep steps [s0, s1) of one staged window (front step s at F[s], back
+// step s at B[s]).
+template <bool kCheck>
+__device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt *B, int s0, int s1,
+                                              int nbk, int eo, float q, float floor_hat,
+                                              const BdyCtx &bc, const BinCtx &b, DevFlags *flags,
+                                              ProjChain &fr, ProjChain &bk, double &I0,
+                                              double &In) {
+    float chi, t_, chi2, t2;
+    int s = s0;
+    if (s == 0) {
+        staged_eval<kCheck>(F, eo, q, floor_hat, chi, t_);
+        fr.start(chi, t_, F->dzh);
+        I0 = boundary_intensity(bc, (1.0 + (double)F->delta) * b.nu_o, F->cell, flags);
+        if (nbk > 0) {
+            staged_eval<kCheck>(B, eo, q, floor_hat, chi, t_);
+            bk.start(chi, t_, B->dzh);
+            In = boundary_intensity(bc, (1.0 + (double)B->delta) * b.nu_o, B->cell, flags);
+        }
+        s = 1;
+    }
+    if (s == 1 && s < s1) {
+        staged_eval<kCheck>(F + 1, eo, q, floor_hat, chi, t_);
+        fr.first(chi, t_, F[1].dzh, I0);
+        if (nbk > 1) {
+            staged_eval<kCheck>(B + 1, eo, q, floor_hat, chi, t_);
+            bk.first(chi, t_, B[1].dzh, In);
+        }
+        s = 2;
+    }
+    // both halves
+    const int e1 = min(s1, nbk);
+    for (; s + 1 < e1; s += 2) {
+        staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
+        staged_eval<kCheck>(B + s, eo, q, floor_hat, chi2, t2);
+        fr.step(chi, t_, F[s].dzh);
+        bk.step(chi2, t2, B[s].dzh);
+        staged_eval<kCheck>(F + s + 1, eo, q, floor_hat, chi, t_);
+        staged_eval<kCheck>(B + s + 1, eo, q, floor_hat, chi2, t2);
+        fr.step(chi, t_, F[s + 1].dzh);
+        bk.step(chi2, t2, B[s + 1].dzh);
+        fr.renorm();
+        bk.renorm();
+    }
+    if (s < e1) {
+        staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
+        staged_eval<kCheck>(B + s, eo, q, floor_hat, chi2, t2);
+        fr.step(chi, t_, F[s].dzh);
+        bk.step(chi2, t2, B[s].dzh);
+        fr.renorm();
+        bk.renorm();
+        s++;
+    }
+    // the rest of the front half
+    for (; s + 1 < s1; s += 2) {
+        staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
+        fr.step(chi, t_, F[s].dzh);
+        staged_eval<kCheck>(F + s + 1, eo, q, floor_hat, chi, t_);
+        fr.step(chi, t_, F[s + 1].dzh);
+        fr.renorm();
+    }
+    if (s < s1) {
+        staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
+        fr.step(chi, t_, F[s].dzh);
+        fr.renorm();
+    }
+}
+
 // u and L at the origin for one (pair, bin): the warp stages the two halves
 // window by window (kStageSteps steps of each), step s of the front being
 // its point nfr-1-s (the far end first) and likewise for the back; each
 // lane eliminates both halves toward the origin, in lock step while both
-// have points.
+// have points.  A window with a line whose inverted opacity can take chi
+// below half the floor runs the checking variant of the sweep.
 __device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, const float2 *ek,
                                             int K, int k0, int k1, int64_t ofr, int nfr,
                                             int64_t obk, int nbk, int eo, float q, float floor_hat,
@@ -692,85 +777,32 @@ __device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, c
     const float neg_cut = -0.499f * floor_hat;
     ProjChain fr, bk;
     double I0 = 0.0, In = 0.0;
-    float chi, t_, chi2, t2;
     for (int s0 = 0; s0 < nfr; s0 += kStageSteps) {
         const int s1 = min(s0 + kStageSteps, nfr);
         const int nF = s1 - s0;
         const int nB = max(0, min(s1, nbk) - s0);
+        bool inverted = false;
         for (int j = lane; j < nF + nB; j += 32) {
             const bool front = j < nF;
             const int st = s0 + (front ? j : j - nF);
             const int64_t gi = front ? ofr + (nfr - 1 - st) : obk + (nbk - 1 - st);
             const float4 v = __ldg(reinterpret_cast<const float4 *>(t.mp) + gi);
             const unsigned cell = (unsigned)__float_as_int(v.x);
-            float2 e0 = __ldg(ek + cell * K + k0);
-            float2 e1 = __ldg(ek + cell * K + k1);
-            if (e0.y < neg_cut) e0.x = __int_as_float(0x7fc00000);
-            if (e1.y < neg_cut) e1.x = __int_as_float(0x7fc00000);
+            const float2 e0 = __ldg(ek + cell * K + k0);
+            const float2 e1 = __ldg(ek + cell * K + k1);
+            inverted |= (e0.y < neg_cut) | (e1.y < neg_cut);
             float4 *dst = reinterpret_cast<float4 *>(buf + (front ? j : kStageSteps + (j - nF)));
             dst[0] = make_float4(v.y, 0.5f * v.z, v.w * kSqrtLog2e, v.x);
             dst[1] = make_float4(e0.x, e0.y, e1.x, e1.y);
         }
+        const bool check = __any_sync(0xffffffffu, inverted);
         __syncwarp();
         const StagedPt *F = buf - s0;                 // front step s at F[s]
         const StagedPt *B = buf + kStageSteps - s0;   // back step s at B[s]
-        int s = s0;
-        if (s == 0) {
-            staged_eval(F, eo, q, floor_hat, chi, t_);
-            fr.start(chi, t_, F->dzh);
-            I0 = boundary_intensity(bc, (1.0 + (double)F->delta) * b.nu_o, F->cell, flags);
-            if (nbk > 0) {
-                staged_eval(B, eo, q, floor_hat, chi, t_);
-                bk.start(chi, t_, B->dzh);
-                In = boundary_intensity(bc, (1.0 + (double)B->delta) * b.nu_o, B->cell, flags);
-            }
-            s = 1;
-        }
-        if (s == 1 && s < s1) {
-            staged_eval(F + 1, eo, q, floor_hat, chi, t_);
-            fr.first(chi, t_, F[1].dzh, I0);
-            if (nbk > 1) {
-                staged_eval(B + 1, eo, q, floor_hat, chi, t_);
-                bk.first(chi, t_, B[1].dzh, In);
-            }
-            s = 2;
-        }
-        // both halves
-        const int e1 = min(s1, nbk);
-        for (; s + 1 < e1; s += 2) {
-            staged_eval(F + s, eo, q, floor_hat, chi, t_);
-            staged_eval(B + s, eo, q, floor_hat, chi2, t2);
-            fr.step(chi, t_, F[s].dzh);
-            bk.step(chi2, t2, B[s].dzh);
-            staged_eval(F + s + 1, eo, q, floor_hat, chi, t_);
-            staged_eval(B + s + 1, eo, q, floor_hat, chi2, t2);
-            fr.step(chi, t_, F[s + 1].dzh);
-            bk.step(chi2, t2, B[s + 1].dzh);
-            fr.renorm();
-            bk.renorm();
-        }
-        if (s < e1) {
-            staged_eval(F + s, eo, q, floor_hat, chi, t_);
-            staged_eval(B + s, eo, q, floor_hat, chi2, t2);
-            fr.step(chi, t_, F[s].dzh);
-            bk.step(chi2, t2, B[s].dzh);
-            fr.renorm();
-            bk.renorm();
-            s++;
-        }
-        // the rest of the front half
-        for (; s + 1 < s1; s += 2) {
-            staged_eval(F + s, eo, q, floor_hat, chi, t_);
-            fr.step(chi, t_, F[s].dzh);
-            staged_eval(F + s + 1, eo, q, floor_hat, chi, t_);
-            fr.step(chi, t_, F[s + 1].dzh);
-            fr.renorm();
-        }
-        if (s < s1) {
-            staged_eval(F + s, eo, q, floor_hat, chi, t_);
-            fr.step(chi, t_, F[s].dzh);
-            fr.renorm();
-        }
+        if (check)
+            staged_window<true>(F, B, s0, s1, nbk, eo, q, floor_hat, bc, b, flags, fr, bk, I0, In);
+        else
+            staged_window<false>(F, B, s0, s1, nbk, eo, q, floor_hat, bc, b, flags, fr, bk, I0, In);
         __syncwarp();
     }
     // the origin row

@@ -45,7 +45,7 @@ def loss_and_grad(params, mean, istd, X, lte, tgt):
     z = lte.astype(np.float64) + delta
     c = np.log(np.exp(z - z.max(1, keepdims=True)).sum(1, keepdims=True)) + z.max(1, keepdims=True)
     r = z - c - tgt
-    w = np.where(tgt > np.log(1e-8), 1.0, 0.1)
+    w = np.where(tgt > np.log(1e-8), 1.0, np.where(tgt > np.log(1e-12), 0.1, 0.0))
     loss = float((w * r * r).sum())
     sm = np.exp(z - c)
     g = 2.0 * (w * r - sm * (w * r).sum(1, keepdims=True))

@@ -56,37 +56,51 @@ def _feautrier_matrix(term1, dtau, I0, In):
 
 
 def two_sided_sweep(n_ar, term1, dtau, I0, In):
-    """The device's algorithm (magritte_b200/csrc/solve.cu, sweep_fp64):
-    front eliminated toward the origin, back toward the origin, joined in
-    the origin's row, with F' = F/(1+F) and G' = G/(1+G)."""
+    """The device's elimination (magritte_b200/csrc/solve.cu, Chain and
+    ProjChain): the front half is eliminated from its far end toward the
+    origin and the back half from its far end toward the origin, on half
+    optical depths dh = dtau/2 in projective form F~ = a/b, S~ = c/b with a
+    power-of-two rescaling after each step, and the halves meet in the
+    origin's row."""
+    import math
     last = term1.shape[0] - 1
     o = n_ar
-    d0 = dtau[0]
-    D = 1.0 / (d0 * d0 + 2 * d0 + 2)
-    Fp, Su = (d0 * d0 + 2 * d0) * D, (term1[0] * d0 * d0 + 2 * I0 * d0) * D
-    for n in range(1, o):
-        h = 0.5 * (dtau[n - 1] + dtau[n])
-        iA, iC = h * dtau[n - 1], h * dtau[n]
-        D = 1.0 / (iA * (1 + iC) + iC * Fp)
-        Su = (term1[n] * iA + Su) * D * iC
-        Fp = iC * (iA + Fp) * D
+
+    def half(idx_far_to_origin, dh_list, I):
+        # idx: point indices from the far end to the point next to the origin
+        t_far = term1[idx_far_to_origin[0]]
+        dh = dh_list[0]
+        a = dh * (dh + 1.0)
+        b = 2.0 * a + 1.0
+        c = dh * (t_far * dh + I)
+        dp = dh
+        for k in range(1, len(dh_list)):
+            dh = dh_list[k]
+            t = term1[idx_far_to_origin[k]]
+            H = dp + dh
+            P, Q = H * dp, H * dh
+            Pb = P * b
+            a = Q * (Pb + a)
+            c = Q * (t * Pb + c)
+            b = 2.0 * a + Pb
+            sc = 2.0 ** -(math.frexp(b)[1] - 1)
+            a, b, c = a * sc, b * sc, c * sc
+            dp = dh
+        return a, b, c, dp
+
+    # front: points 0 .. o-1, segment n between n and n+1
+    af, bf, cf, df = half(list(range(0, o)), [0.5 * dtau[n] for n in range(0, o)], I0)
+    to = term1[o]
     if o == last:
-        d = dtau[last - 1]
-        den = 1.0 / (d * d + 2 * d + 2 * Fp)
-        return (term1[o] * d * d + 2 * In * d + 2 * Su) * den, d * d * den
-    d = dtau[last - 1]
-    D = 1.0 / (d * d + 2 * d + 2)
-    Gp, Sb = (d * d + 2 * d) * D, (term1[last] * d * d + 2 * In * d) * D
-    for n in range(last - 1, o, -1):
-        h = 0.5 * (dtau[n - 1] + dtau[n])
-        iA, iC = h * dtau[n - 1], h * dtau[n]
-        D = 1.0 / (iC * (1 + iA) + iA * Gp)
-        Sb = (term1[n] * iC + Sb) * D * iA
-        Gp = iA * (iC + Gp) * D
-    h = 0.5 * (dtau[o - 1] + dtau[o])
-    iA, iC = h * dtau[o - 1], h * dtau[o]
-    den = 1.0 / (iA * iC + Fp * iC + Gp * iA)
-    return (term1[o] * iA * iC + Su * iC + Sb * iA) * den, iA * iC * den
+        D = 1.0 / (df * (df + 1.0) * bf + af)
+        return (df * (to * df + In) * bf + cf) * D, df * df * bf * D
+    ab, bb, cb, db = half(list(range(last, o, -1)),
+                          [0.5 * dtau[n] for n in range(last - 1, o - 1, -1)], In)
+    H = df + db
+    P, Q = H * df, H * db
+    PQB = P * Q * (bf * bb)
+    D = 1.0 / (af * bb * Q + ab * bf * P + PQB)
+    return (to * PQB + cf * bb * Q + cb * bf * P) * D, PQB * D
 
 
 @pytest.mark.parametrize("n_ar,n_r", [(5, 5), (1, 0), (1, 1), (2, 1), (7, 0), (12, 3), (30, 29)])
