@@ -66,6 +66,11 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="default solve kernel shapes")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end repeat (for workloads whose solve takes minutes)")
+    ap.add_argument("--max-iter", type=int, default=MAX_ITER,
+                    help="ALI iteration cap (a batch stops when every model converged or at the cap)")
+    ap.add_argument("--plain-max-iter", type=int, default=None,
+                    help="iteration cap of the plain FP64 solve (default: --max-iter); a plain "
+                         "solve stopped by the cap reports converged: false and a lower bound")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -310,11 +315,11 @@ def run_b200(args):
         else:
             sim.compute_LTE_level_populations()
 
-    def one_solve(sim, learned=net is not None, precision=prec):
+    def one_solve(sim, learned=net is not None, precision=prec, max_iter=None):
         sim.trace()
         start(sim, learned)
-        return sim.compute_level_populations(True, MAX_ITER, precision, tol_max_rel=TOL,
-                                             use_graph=graph)
+        return sim.compute_level_populations(True, max_iter or args.max_iter, precision,
+                                             tol_max_rel=TOL, use_graph=graph)
 
     # ---- device-resident solve
     sim = Simulation(model, device=local if dist else 0)
@@ -324,7 +329,7 @@ def run_b200(args):
     sim.compute_boundary_intensities()
     for _ in range(args.warmup):
         one_solve(sim)
-    if not args.no_plain:
+    if not args.no_plain and not args.no_autotune:
         # tune the FP64 kernel before the plain solve is timed
         sim.trace()
         start(sim, False)
@@ -349,8 +354,10 @@ def run_b200(args):
     if model.meta.get("segments"):
         import numpy as np
         _, mit = sim.segment_results()
+        mst, _ = sim.segment_results()
         model_iters = {"min": int(mit.min()), "median": float(np.median(mit)),
-                       "max": int(mit.max()), "sum": int(mit.sum())}
+                       "max": int(mit.max()), "sum": int(mit.sum()),
+                       "not_converged": [int(i) for i in np.nonzero(~(mst[:, 2] < TOL))[0]]}
     tuning = sim.tuning(prec) if not args.no_autotune else None
     err_hist = list(sim.error_max)
     t_step = statistics.mean(times)
@@ -367,7 +374,7 @@ def run_b200(args):
         start(s2, net is not None)
         if not args.no_autotune:
             s2.set_autotune(True)
-        s2.compute_level_populations(True, MAX_ITER, prec, tol_max_rel=TOL, use_graph=graph)
+        s2.compute_level_populations(True, args.max_iter, prec, tol_max_rel=TOL, use_graph=graph)
         pop = s2.population
         e2e.append(time.perf_counter() - t0)
         s2.close()
@@ -377,11 +384,15 @@ def run_b200(args):
     # ---- the plain method: FP64 from the LTE start (north-star comparison)
     plain = None
     if not args.no_plain:
+        print(json.dumps({"progress": "headline step done", "seconds": times, "iterations": iters,
+                          "converged": converged, "history": err_hist}), file=sys.stderr,
+              flush=True)
         sim.timer_start()
-        it_p = one_solve(sim, learned=False, precision="fp64")
+        it_p = one_solve(sim, learned=False, precision="fp64", max_iter=args.plain_max_iter)
         t_p = sim.timer_stop() / 1e3
         plain = {"start": "LTE", "precision": "fp64", "ali_iterations": it_p, "seconds": t_p,
-                 "converged": bool(getattr(sim, "converged", False))}
+                 "converged": bool(getattr(sim, "converged", False)),
+                 "final_max_rel_change": sim.error_max[-1] if sim.error_max else None}
         if model.meta.get("segments"):
             import numpy as np
             _, mit = sim.segment_results()

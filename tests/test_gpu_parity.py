@@ -172,3 +172,30 @@ def test_ali_mixed_populations(gpu):
     assert sim.converged
     orc.compute_level_populations(True, 300, 1e-7)
     assert rel_err(sim.population, orc.pop) < MIXED_RTOL
+
+
+def test_mixed_patches_inverted_lines(gpu):
+    """Populations inverted in a block of cells: the mixed solve sends the
+    affected (origin, pair, bin) solves to the double-precision patch pass
+    and still agrees with the FP64 solve to 1e-4; the FP64 solve agrees with
+    the oracle."""
+    model = small_wind(10, 5, 7)
+    sim, orc = setup_pair(model, keep_J=False)
+    pop = sim.population.copy()
+    ld = model.linedata
+    i, j = int(ld.irad[0]), int(ld.jrad[0])
+    g = ld.weight
+    # cells 100..399: upper level of line 0 over-populated (n_i/g_i > n_j/g_j)
+    cells = slice(100, 400)
+    pop[cells, i] = 5.0 * pop[cells, j] * g[i] / g[j]
+    pop[cells] *= (model.population_tot[cells] / pop[cells].sum(1))[:, None]
+    sim.population = pop
+    orc.set_populations(pop)
+    sim.compute_radiation_field("fp64", keep_J=True)
+    J64, L64 = sim.J.copy(), sim.Lambda.copy()
+    orc.compute_radiation_field()
+    assert rel_err(J64, orc.J, floor=1e-10 * np.abs(orc.J).max()) < FP64_RTOL
+    sim.compute_radiation_field("mixed", keep_J=True)
+    patched, fallbacks = sim.patch_stats()
+    assert patched > 0 and fallbacks == 0
+    assert rel_err(sim.J, J64, floor=1e-6 * np.abs(J64).max()) < MIXED_RTOL

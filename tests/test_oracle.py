@@ -398,3 +398,21 @@ def test_concat_models_keeps_each_member():
                 assert np.array_equal(shb, shm) and np.array_equal(dzb, dzm)
     with pytest.raises(ValueError):
         M.concat_models([ms[0], M.wind_model(4, seed=9, nlev=4, npairs=3)])
+
+
+def test_two_sided_sweep_with_inverted_segments():
+    """Masing segments (negative optical depth, allowed by the reference's
+    iteration): the device's elimination still solves the reference's
+    system."""
+    rng = np.random.default_rng(11)
+    for _ in range(300):
+        n_ar, n_r = int(rng.integers(1, 30)), int(rng.integers(0, 30))
+        ndep = n_ar + n_r + 1
+        term1 = rng.uniform(-2.0, 2.0, ndep)
+        sign = np.where(rng.random(ndep - 1) < 0.2, -1.0, 1.0)
+        dtau = sign * rng.uniform(0.1, 3.0, ndep - 1) * 10 ** rng.uniform(-3, 2)
+        I0, In = rng.uniform(0, 1, 2)
+        u, L = oracle.solve_raypair(n_ar, term1, dtau, I0, In)
+        u2, L2 = two_sided_sweep(n_ar, term1, dtau, I0, In)
+        assert abs(u2 - u) <= 1e-9 * abs(u) + 1e-300
+        assert abs(L2 - L) <= 1e-9 * abs(L) + 1e-300
