@@ -87,6 +87,7 @@ struct mgr_handle {
     double updates_per_solve = 0.0;
     int max_pair_points = 0;
     std::vector<int32_t> h_len;        // [nrays*N] host copy for npoints
+    std::vector<float> upd_origin;     // [N] updates of one formal solve per origin (batches)
 
     bool model_loaded = false, line_set = false, bdy_set = false, pops_valid = false;
     bool keep_J = false;
@@ -569,6 +570,8 @@ void do_trace(mgr_handle *h) {
     double U = 0.0;
     int64_t total = 0;
     std::vector<int64_t> per_origin(N, 0);
+    if (h->nseg > 0) h->upd_origin.assign(N, 0.0f);
+    else h->upd_origin.clear();
     for (int64_t d = 0; d < R; d++)
         for (int64_t o = 0; o < N; o++) {
             total += h->h_len[d * N + o];
@@ -578,7 +581,10 @@ void do_trace(mgr_handle *h) {
         const int64_t ar = h->antipod[r];
         for (int64_t o = 0; o < N; o++) {
             const int64_t ndep = (int64_t)h->h_len[r * N + o] + h->h_len[ar * N + o] + 1;
-            if (ndep > 1) U += (double)ndep;
+            if (ndep > 1) {
+                U += (double)ndep;
+                if (h->nseg > 0) h->upd_origin[o] += (float)(ndep * h->nfreqs);
+            }
             h->max_pair_points = std::max<int>(h->max_pair_points, (int)(ndep - 1));
         }
     }
@@ -795,6 +801,17 @@ void finish_solve(mgr_handle *h, int precision, int variant, bool timing, int64_
     if (timing) tune_record(h, precision, variant, ms);
     h->last_solve_ms = ms;
     h->last_updates = h->updates_per_solve;
+    if (h->nseg > 0 && (int64_t)h->upd_origin.size() == h->N) {
+        // a batch: only the origins of models still iterating were solved
+        std::vector<int64_t> sb(h->nseg + 1);
+        ck(cudaMemcpy(sb.data(), h->seg_begin_d, (h->nseg + 1) * sizeof(int64_t),
+                      cudaMemcpyDeviceToHost), "model bounds");
+        double U = 0.0;
+        for (int64_t g = 0; g < h->nseg; g++)
+            if (h->h_seg_active[g])
+                for (int64_t o = sb[g]; o < sb[g + 1]; o++) U += h->upd_origin[o];
+        h->last_updates = U;
+    }
     h->last_patched = patched;
 }
 
@@ -1230,6 +1247,7 @@ mgr_status mgr_set_segments(mgr_handle *h, int64_t nseg, const int64_t *seg_begi
                       cudaMemcpyHostToDevice), "upload");
         h->nseg = nseg;
         h->seg_iters.assign(nseg, 0);
+        h->traced = false;   // the next trace also counts each model's updates
         h->mv.nseg = nseg;
         h->mv.seg_begin = h->seg_begin_d;
         h->mv.cell_seg = h->cell_seg_d;
