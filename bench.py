@@ -46,7 +46,7 @@ METRIC = "ALI iters & wall-clock to 1e-4 pops on 1 B200: learned+FP32 vs plain F
 TOL = 1.0e-4
 MAX_ITER = 400
 FALLBACK_HBM_GBS = 6650.0
-STAGED_DRAM_BYTES_PER_UPDATE = 0.535
+STAGED_DRAM_BYTES_PER_UPDATE = 0.556
 
 
 def parse():
