@@ -37,6 +37,8 @@
 // (Simulation::compute_Jeff, sim_lines.tpp:185-198) and the diagonal ALO
 // Lam[o][k] (RayPair::update_Lambda, raypair_lambda.tpp:94-149), both
 // reduced over the bins of a line with warp shuffles; optionally J itself.
+#include <type_traits>
+
 #include "mgr_internal.cuh"
 
 namespace mgr {
@@ -651,16 +653,19 @@ __device__ __forceinline__ void staged_eval(const StagedPt *p, int eo, float q, 
 // multiplied through by b).  Every term is non-negative for non-negative
 // opacities, so nothing cancels; a, b, c are rescaled by a power of two
 // every second step, which keeps them in range for any optical depth.
-struct ProjChain {
-    float chi_a, t_a, dzh_a;   // current point
+// R is the type of the staged point values (float in mixed precision,
+// double in FP64); the elimination itself is always double.
+template <class R>
+struct ProjChainT {
+    R chi_a, t_a, dzh_a;   // current point
     double dh_prev, a, b, c;
 
-    __device__ __forceinline__ void start(float chi, float t, float dzh) {
+    __device__ __forceinline__ void start(R chi, R t, R dzh) {
         chi_a = chi; t_a = t; dzh_a = dzh;
     }
     // boundary row of the far end: F~ = dh(dh+1)/(2dh(dh+1)+1),
     // S~ = dh(t dh + I)/(2dh(dh+1)+1)
-    __device__ __forceinline__ void first(float chi_b, float t_b, float dzh_b, double I) {
+    __device__ __forceinline__ void first(R chi_b, R t_b, R dzh_b, double I) {
         const double dh = (double)((chi_a + chi_b) * dzh_a);
         a = dh * (dh + 1.0);
         b = fma(2.0, a, 1.0);
@@ -668,7 +673,7 @@ struct ProjChain {
         dh_prev = dh;
         chi_a = chi_b; t_a = t_b; dzh_a = dzh_b;
     }
-    __device__ __forceinline__ void step(float chi_b, float t_b, float dzh_b) {
+    __device__ __forceinline__ void step(R chi_b, R t_b, R dzh_b) {
         const double dh = (double)((chi_a + chi_b) * dzh_a);
         const double H = dh_prev + dh;
         const double P = H * dh_prev, Q = H * dh;
@@ -684,6 +689,7 @@ struct ProjChain {
         a *= sc; b *= sc; c *= sc;
     }
 };
+using ProjChain = ProjChainT<float>;
 
 // Steps of the sweep held in shared memory at a time (per half).
 #ifndef MGR_STAGE_STEPS
@@ -831,7 +837,161 @@ __device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, c
     L = PQB * D;
 }
 
-template <int kMinBlocks>
+// ------------------------------------------------------------------ staged FP64 solve
+//
+// The FP64 solve with the same staging: per window the warp gathers each
+// point's shift, dZ/4, profile width and its inverse, and the (eps, kap) of
+// the chunk's two lines; each lane then evaluates emissivity and opacity
+// exactly as Simulation::get_eta_and_chi does (simulation.tpp:385-481, its
+// own line only: the lines' windows do not overlap) and eliminates in the
+// same projective form.
+
+struct __align__(8) StagedPt64 {
+    double shift, dzq, pw, inv_pw;   // dzq = dZ / 4: dh = (chi_a + chi_b) dzq
+    double e[4];                     // eps, kap of the chunk's first and second line
+    int64_t cell;
+};
+
+constexpr int kStageSteps64 = 32;
+
+struct Lane64 {
+    double nu_o, line, inv_line;
+    int eo;   // 0 or 2: this lane's line in StagedPt64::e
+};
+
+__device__ __forceinline__ void staged_eval64(const StagedPt64 *p, const Lane64 &l, double &chi,
+                                              double &t) {
+    const double freq = p->shift * l.nu_o;
+    const double width = l.line * p->pw;
+    const double diff = freq - l.line;
+    const bool in = diff <= 11.0 * width && diff >= -11.0 * width;
+    const double inv_w = l.inv_line * p->inv_pw;
+    const double x = inv_w * diff;
+    const double fp = in ? freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x))) : 0.0;
+    const double eta = p->e[l.eo] * fp;
+    chi = 1.0E-26 + p->e[l.eo + 1] * fp;
+    t = eta * rcp_pos(chi);
+}
+
+__device__ __forceinline__ void staged_window64(const StagedPt64 *F, const StagedPt64 *B, int s0,
+                                                int s1, int nbk, const Lane64 &ln,
+                                                const BdyCtx &bc, DevFlags *flags,
+                                                ProjChainT<double> &fr, ProjChainT<double> &bk,
+                                                double &I0, double &In) {
+    double chi, t_, chi2, t2;
+    int s = s0;
+    if (s == 0) {
+        staged_eval64(F, ln, chi, t_);
+        fr.start(chi, t_, F->dzq);
+        I0 = boundary_intensity(bc, F->shift * ln.nu_o, (int)F->cell, flags);
+        if (nbk > 0) {
+            staged_eval64(B, ln, chi, t_);
+            bk.start(chi, t_, B->dzq);
+            In = boundary_intensity(bc, B->shift * ln.nu_o, (int)B->cell, flags);
+        }
+        s = 1;
+    }
+    if (s == 1 && s < s1) {
+        staged_eval64(F + 1, ln, chi, t_);
+        fr.first(chi, t_, F[1].dzq, I0);
+        if (nbk > 1) {
+            staged_eval64(B + 1, ln, chi, t_);
+            bk.first(chi, t_, B[1].dzq, In);
+        }
+        s = 2;
+    }
+    const int e1 = min(s1, nbk);
+    for (; s + 1 < e1; s += 2) {
+        staged_eval64(F + s, ln, chi, t_);
+        staged_eval64(B + s, ln, chi2, t2);
+        fr.step(chi, t_, F[s].dzq);
+        bk.step(chi2, t2, B[s].dzq);
+        staged_eval64(F + s + 1, ln, chi, t_);
+        staged_eval64(B + s + 1, ln, chi2, t2);
+        fr.step(chi, t_, F[s + 1].dzq);
+        bk.step(chi2, t2, B[s + 1].dzq);
+        fr.renorm();
+        bk.renorm();
+    }
+    if (s < e1) {
+        staged_eval64(F + s, ln, chi, t_);
+        staged_eval64(B + s, ln, chi2, t2);
+        fr.step(chi, t_, F[s].dzq);
+        bk.step(chi2, t2, B[s].dzq);
+        fr.renorm();
+        bk.renorm();
+        s++;
+    }
+    for (; s + 1 < s1; s += 2) {
+        staged_eval64(F + s, ln, chi, t_);
+        fr.step(chi, t_, F[s].dzq);
+        staged_eval64(F + s + 1, ln, chi, t_);
+        fr.step(chi, t_, F[s + 1].dzq);
+        fr.renorm();
+    }
+    if (s < s1) {
+        staged_eval64(F + s, ln, chi, t_);
+        fr.step(chi, t_, F[s].dzq);
+        fr.renorm();
+    }
+}
+
+__device__ __forceinline__ void staged_pair64(StagedPt64 *buf, const TraceView &t, const double *eps,
+                                              const double *kap, int K, int k0, int k1, int64_t ofr,
+                                              int nfr, int64_t obk, int nbk, const Lane64 &ln,
+                                              const BdyCtx &bc, const BinCtx &b, double chi_o,
+                                              double t_o, const ModelView &m, int origin, int lane,
+                                              DevFlags *flags, double &u, double &L) {
+    ProjChainT<double> fr, bk;
+    double I0 = 0.0, In = 0.0;
+    for (int s0 = 0; s0 < nfr; s0 += kStageSteps64) {
+        const int s1 = min(s0 + kStageSteps64, nfr);
+        const int nF = s1 - s0;
+        const int nB = max(0, min(s1, nbk) - s0);
+        for (int j = lane; j < nF + nB; j += 32) {
+            const bool front = j < nF;
+            const int st = s0 + (front ? j : j - nF);
+            const int64_t gi = front ? ofr + (nfr - 1 - st) : obk + (nbk - 1 - st);
+            const int cell = __ldg(t.cell + gi);
+            StagedPt64 *d = buf + (front ? j : kStageSteps64 + (j - nF));
+            d->shift = __ldg(t.shift + gi);
+            d->dzq = 0.25 * __ldg(t.dZ + gi);
+            d->pw = __ldg(m.pw + cell);
+            d->inv_pw = __ldg(m.inv_pw + cell);
+            d->e[0] = __ldg(eps + (unsigned)cell * K + k0);
+            d->e[1] = __ldg(kap + (unsigned)cell * K + k0);
+            d->e[2] = __ldg(eps + (unsigned)cell * K + k1);
+            d->e[3] = __ldg(kap + (unsigned)cell * K + k1);
+            d->cell = cell;
+        }
+        __syncwarp();
+        staged_window64(buf - s0, buf + kStageSteps64 - s0, s0, s1, nbk, ln, bc, flags, fr, bk, I0,
+                        In);
+        __syncwarp();
+    }
+    if (nfr == 1) fr.first(chi_o, t_o, 0.0, I0);
+    else fr.step(chi_o, t_o, 0.0);
+    if (nbk == 0) {
+        const int bo = __ldg(m.cell2bdy + origin);
+        if (bo >= 0) In = __ldg(m.ibdy + (int64_t)bo * m.nfreqs + b.f);
+        else atomicAdd(&flags->trace_err, 1ull);
+        const double dh = fr.dh_prev;
+        const double D = rcp_pos(fma(dh * (dh + 1.0), fr.b, fr.a));
+        u = fma(dh * fma(t_o, dh, In), fr.b, fr.c) * D;
+        L = dh * dh * fr.b * D;
+        return;
+    }
+    if (nbk == 1) bk.first(chi_o, t_o, 0.0, In);
+    else bk.step(chi_o, t_o, 0.0);
+    const double H = fr.dh_prev + bk.dh_prev;
+    const double P = H * fr.dh_prev, Q = H * bk.dh_prev;
+    const double PQB = P * Q * (fr.b * bk.b);
+    const double D = rcp_pos(fma(fr.a * bk.b, Q, fma(bk.a * fr.b, P, PQB)));
+    u = fma(t_o, PQB, fma(fr.c * bk.b, Q, bk.c * fr.b * P)) * D;
+    L = PQB * D;
+}
+
+template <int kMinBlocks, bool kFp64>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -841,9 +1001,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     const int o = (int)(t.o_begin + oi);
     if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
-    constexpr int cap = 2 * kStageSteps;
-    StagedPt *pts = reinterpret_cast<StagedPt *>(smem_raw) + (size_t)warp * cap;
-    double *sJ = reinterpret_cast<double *>(reinterpret_cast<StagedPt *>(smem_raw) +
+    using Pt = typename std::conditional<kFp64, StagedPt64, StagedPt>::type;
+    constexpr int cap = 2 * (kFp64 ? kStageSteps64 : kStageSteps);
+    Pt *pts = reinterpret_cast<Pt *>(smem_raw) + (size_t)warp * cap;
+    double *sJ = reinterpret_cast<double *>(reinterpret_cast<Pt *>(smem_raw) +
                                             (size_t)kWarpsPerBlock * cap) + (size_t)warp * 2 * K;
     double *sL = sJ + K;
     for (int k = lane; k < K; k += 32) { sJ[k] = 0.0; sL[k] = 0.0; }
@@ -870,12 +1031,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
         const int k1 = min(K - 1, k0 + 1);
         const int eo = b.k != k0 ? 3 : 2;   // float2 index of this lane's line in a StagedPt
 
-        // origin in double; an inverted line taking chi below half the floor
-        // there poisons the bin
+        // origin in double; in mixed precision an inverted line taking chi
+        // below half the floor there poisons the bin
         double e64, c64;
         eta_chi_double(m, a.eps, a.kap, o, b.nu_o, b.k, b.k, e64, c64);
         const float chi_o = (float)(c64 * m.mixed_scale);
         const float t_o = c64 < 0.5E-26 ? __int_as_float(0x7fc00000) : (float)(e64 / c64);
+        const double t_o64 = e64 * rcp_pos(c64);
+        Lane64 ln;
+        ln.nu_o = b.nu_o;
+        ln.line = line_k;
+        ln.inv_line = m.inv_line[b.k];
+        ln.eo = b.k != k0 ? 2 : 0;
         const double width_o = line_k * pw_o;
         const double iw = 1.0 / width_o;
         const double xo = iw * (b.nu_o - line_k);
@@ -903,9 +1070,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
                 continue;
             }
             double u, L;
-            staged_pair(pts, t, ek, K, k0, k1, ofr, nfr, obk, nbk, eo, b.q, floor_hat, bc, b, chi_o,
-                        t_o, m, o, lane, flags, u, L);
-            if (!(isfinite(u) && isfinite(L))) {
+            if constexpr (kFp64) {
+                staged_pair64(pts, t, a.eps, a.kap, K, k0, k1, ofr, nfr, obk, nbk, ln, bc, b, c64,
+                              t_o64, m, o, lane, flags, u, L);
+            } else {
+                staged_pair(pts, t, ek, K, k0, k1, ofr, nfr, obk, nbk, eo, b.q, floor_hat, bc, b,
+                            chi_o, t_o, m, o, lane, flags, u, L);
+            }
+            if (!kFp64 && !(isfinite(u) && isfinite(L))) {
                 const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
                 if (slot < (unsigned long long)a.patch_cap) a.patch[slot] = make_int4(o, r, fc, 0);
                 else atomicAdd(&flags->patch_overflow, 1ull);
@@ -944,7 +1116,9 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
     if (t.o_count == 0) return cudaSuccess;
     const int64_t blocks = (t.o_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const size_t shmem = (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
-    const bool staged = precision == MGR_MIXED && !m.overlap && m.nquads >= 31;
+    // the staged kernels need each 32-bin chunk within two lines and lines
+    // whose windows do not overlap
+    const bool staged = !m.overlap && m.nquads >= 31;
     if (kind) *kind = staged ? 1 : 0;
     if (variant < 0 || variant >= kSolveVariants) variant = staged ? kDefaultStaged : kDefaultGeneric;
     auto run = [&](auto pol) {
@@ -976,7 +1150,9 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         run(pol);
     };
     if (staged) {
-        const size_t sm = (size_t)kWarpsPerBlock * 2 * kStageSteps * sizeof(StagedPt) +
+        const bool f64 = precision == MGR_FP64;
+        const size_t sm = (f64 ? (size_t)kWarpsPerBlock * 2 * kStageSteps64 * sizeof(StagedPt64)
+                               : (size_t)kWarpsPerBlock * 2 * kStageSteps * sizeof(StagedPt)) +
                           (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
         auto go = [&](auto kern) -> cudaError_t {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -986,10 +1162,18 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
             return cudaSuccess;
         };
         cudaError_t e;
-        switch (variant) {
-            case 0: e = go(formal_solve_staged_kernel<kVariantBlocks[0]>); break;
-            case 1: e = go(formal_solve_staged_kernel<kVariantBlocks[1]>); break;
-            default: e = go(formal_solve_staged_kernel<kVariantBlocks[2]>); break;
+        if (f64) {
+            switch (variant) {
+                case 0: e = go(formal_solve_staged_kernel<kVariantBlocks[0], true>); break;
+                case 1: e = go(formal_solve_staged_kernel<kVariantBlocks[1], true>); break;
+                default: e = go(formal_solve_staged_kernel<kVariantBlocks[2], true>); break;
+            }
+        } else {
+            switch (variant) {
+                case 0: e = go(formal_solve_staged_kernel<kVariantBlocks[0], false>); break;
+                case 1: e = go(formal_solve_staged_kernel<kVariantBlocks[1], false>); break;
+                default: e = go(formal_solve_staged_kernel<kVariantBlocks[2], false>); break;
+            }
         }
         if (e != cudaSuccess) return e;
     } else if (precision == MGR_MIXED) {
@@ -1003,7 +1187,7 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
         // solves again in double
         const unsigned pblocks = (unsigned)std::min<int64_t>((a.patch_cap + 127) / 128, 148 * 16);
         patch_kernel<<<pblocks, 128, 0, s>>>(m, t, a, flags);
-    } else {
+    } else if (!staged) {
         if (m.overlap) fp64(Fp64Policy<true>{});
         else fp64(Fp64Policy<false>{});
     }

@@ -94,7 +94,7 @@ def test_autotuner_candidates_agree(gpu, precision):
     t = sim.tuning(precision)
     assert t["tuned"] and all(x > 0 for x in t["ms"])
     assert t["min_blocks"] in (6, 7, 8)
-    assert t["kernel"] == ("staged" if precision == "mixed" else "generic")
+    assert t["kernel"] == "staged"
     for o in outs[1:]:
         for x, y in zip(o, outs[0]):
             assert np.array_equal(x, y)

@@ -199,3 +199,20 @@ def test_mixed_patches_inverted_lines(gpu):
     patched, fallbacks = sim.patch_stats()
     assert patched > 0 and fallbacks == 0
     assert rel_err(sim.J, J64, floor=1e-6 * np.abs(J64).max()) < MIXED_RTOL
+
+
+def test_generic_kernels_few_bins(gpu):
+    """21 bins per line (a 32-bin chunk spans three lines): the generic FP64
+    and mixed kernels run instead of the staged ones; FP64 against the oracle
+    to 1e-6, mixed to 1e-4."""
+    model = M.lattice_cloud(8, nquads=21, name="lattice8_q21")
+    sim, orc = setup_pair(model, keep_J=False)
+    sim.compute_radiation_field("fp64", keep_J=True)
+    orc.compute_radiation_field()
+    orc.compute_Jeff()
+    assert sim.tuning("fp64")["kernel"] == "generic"
+    assert rel_err(sim.J, orc.J) < FP64_RTOL
+    assert rel_err(sim.Lambda, orc.Ls) < FP64_RTOL
+    sim.compute_radiation_field("mixed", keep_J=True)
+    assert sim.tuning("mixed")["kernel"] == "generic"
+    assert rel_err(sim.J, orc.J) < MIXED_RTOL
