@@ -136,17 +136,28 @@ def dist_env():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples, started ahead of the timed region (its start-up
+    is kept out of the timed steps) and summarised over the timed window
+    only (`mark_start` / `mark_end`)."""
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        import datetime
+        self.t0 = datetime.datetime.now()
+
+    def mark_end(self):
+        import datetime
+        self.t1 = datetime.datetime.now()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}",
-                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "--query-gpu=timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "200"],
@@ -165,24 +176,28 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
+        import datetime
+        rows = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in (self.out or "").strip().splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 8:
+            if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[0]))
-                mx.append(float(f[1]))
+                sm, mx = float(f[1]), float(f[2])
             except ValueError:
                 continue
-            for n, v in zip(names, f[4:8]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+            try:
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+                inside = self.t0 is None or self.t1 is None or self.t0 <= ts <= self.t1
+            except ValueError:
+                inside = True
+            rows.append((inside, sm, mx, [n for n, v in zip(names, f[5:9]) if v.lower() == "active"]))
+        sel = [r for r in rows if r[0]] or rows   # every sample if none carries a usable time
+        if not sel:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(r[1] for r in sel), "sm_max_mhz": max(r[2] for r in sel),
+                "reasons": sorted({n for r in sel for n in r[3]}), "samples": len(sel)}
 
 
 def peaks():
@@ -327,7 +342,7 @@ def run_b200(args):
         sim.set_autotune(True)
     sim.compute_spectral_discretisation()
     sim.compute_boundary_intensities()
-    for _ in range(args.warmup):
+    for _ in range(max(0, args.warmup - 1)):
         one_solve(sim)
     if not args.no_plain and not args.no_autotune:
         # tune the FP64 kernel before the plain solve is timed
@@ -337,9 +352,15 @@ def run_b200(args):
             sim.compute_radiation_field("fp64")
     if dist:
         tdist.barrier()
-    launches0 = sim.launch_count()
     times, iters, solve_ms, solve_upd = [], [], [], []
     with Clocks(local) as clk:
+        time.sleep(2.0)          # sampler start-up outside the timed steps
+        if args.warmup > 0:
+            one_solve(sim)       # the last warm-up step, with the sampler running
+        if dist:
+            tdist.barrier()
+        launches0 = sim.launch_count()
+        clk.mark_start()
         for _ in range(args.steps):
             sim.timer_start()
             it = one_solve(sim)
@@ -348,6 +369,7 @@ def run_b200(args):
             ms, up = sim.solve_stats()
             solve_ms.append(ms)
             solve_upd.append(up)
+        clk.mark_end()
     launches = (sim.launch_count() - launches0) // max(1, args.steps)
     converged = bool(getattr(sim, "converged", False))
     model_iters = None
