@@ -589,7 +589,7 @@ void do_trace(mgr_handle *h) {
         }
     }
     h->updates_per_solve = U * h->nfreqs;
-    if (h->max_pair_points != old_max_pair) {   // the kernel choice depends on it
+    if (h->max_pair_points != old_max_pair) {   // tuned shapes depend on the ray lengths
         h->tune[0] = mgr_handle::Tune{};
         h->tune[1] = mgr_handle::Tune{};
     }
@@ -674,7 +674,6 @@ SolveArgs solve_args(mgr_handle *h) {
     a.patch = h->patch;
     a.patch_count = h->patch_count;
     a.patch_cap = h->patch_cap;
-    a.max_pair_points = h->max_pair_points;
     return a;
 }
 
@@ -1283,7 +1282,7 @@ mgr_status mgr_get_tuning(mgr_handle *h, int32_t precision, mgr_tuning *out) {
         const mgr_handle::Tune &tu = h->tune[precision == MGR_MIXED];
         *out = mgr_tuning{};
         out->kernel = tu.kind;
-        const int v = tu.best >= 0 ? tu.best : (tu.kind == 1 ? 2 : 1);
+        const int v = tu.best >= 0 ? tu.best : (tu.kind == 1 && precision == MGR_MIXED ? 2 : 1);
         out->min_blocks = solve_variant_blocks(v);
         out->warps_per_block = 4;
         out->tuned = tu.best >= 0 ? 1 : 0;

@@ -143,7 +143,6 @@ struct SolveArgs {
     double *Jlin, *Lam;             // [N*K]
     double *J;                      // [N*nfreqs] or null
     int warps_per_block;
-    int max_pair_points;            // longest ray pair (both halves) of the trace store
     int4 *patch;                    // mixed: (origin, pair, bin) to redo in double
     unsigned long long *patch_count;
     int64_t patch_cap;

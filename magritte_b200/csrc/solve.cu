@@ -17,14 +17,21 @@
 // origin; the two meet in the origin's row:
 //     u_o  = (S_o + A_o Su_{o-1} + C_o Sb_{o+1}) / (1 + A_o F'_{o-1} + C_o G'_{o+1})
 //     L_oo =                                   1 / (1 + A_o F'_{o-1} + C_o G'_{o+1})
-// with F' = F/(1+F), G' = G/(1+G) the reference's F and G.  This is the same
-// linear system and the same diagonal ALO element (the reference's
-// L_diag[n_ar] = inv_C/(F + G/(1+G))), with O(1) state per lane.  Written
-// with p = (dtau_far + dtau_near) dtau_far / 2 and q = (...) dtau_near / 2,
-// one elimination step toward the origin is, for either half,
-//     D = 1 / (p (1 + q) + q F');  S <- (t p + S) D q;  F' <- q (p + F') D
-// i.e. one reciprocal per point, and the two halves are independent chains
-// that a lane advances together for instruction-level parallelism.
+// with F' = F/(1+F), G' = G/(1+G) the reference's F and G.  This is the
+// same linear system and the same diagonal ALO element (the reference's
+// L_diag[n_ar] = inv_C/(F + G/(1+G))), with O(1) state per lane.  The
+// elimination runs on half optical depths in projective form (F'/2 = a/b,
+// S/2 = c/b), so a step toward the origin needs no division:
+//     H = dh_far + dh_near, P = H dh_far, Q = H dh_near, Pb = P b,
+//     a <- Q (Pb + a),  c <- Q (t Pb + c),  b <- Pb + 2a
+// with a power-of-two rescaling of (a, b, c); the two halves are
+// independent chains that a lane advances together for instruction-level
+// parallelism, and one division per (pair, bin) joins them at the origin.
+//
+// Kernels: the staged kernels (lines whose windows do not overlap, 31 or
+// more bins per line, FP64 or mixed) stage each ray pair's points window by
+// window in shared memory; the generic kernel reads them from the trace
+// store and handles overlapping lines.
 //
 // Precision policies:
 //   FP64  every quantity in double, as the reference.
@@ -48,9 +55,10 @@ namespace {
 constexpr int kWarpsPerBlock = 4;
 // Resident blocks per SM each solve kernel is compiled for (its register
 // budget): the autotuner's candidates.  Defaults when not tuning: 7 for the
-// generic kernel, 8 for the staged one (measured best on the 64^3 wind).
+// generic and the staged FP64 kernels, 8 for the staged mixed one (measured
+// best on the 64^3 wind).
 constexpr int kVariantBlocks[kSolveVariants] = {6, 7, 8};
-constexpr int kDefaultGeneric = 1, kDefaultStaged = 2;
+constexpr int kDefaultGeneric = 1, kDefaultStaged = 2, kDefaultStaged64 = 1;
 
 // 1/x for normal x of either sign: hardware estimate refined by two Newton-Raphson
 // steps y <- y (2 - x y) (accurate to about one ulp).
@@ -1120,7 +1128,8 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
     // whose windows do not overlap
     const bool staged = !m.overlap && m.nquads >= 31;
     if (kind) *kind = staged ? 1 : 0;
-    if (variant < 0 || variant >= kSolveVariants) variant = staged ? kDefaultStaged : kDefaultGeneric;
+    if (variant < 0 || variant >= kSolveVariants)
+        variant = !staged ? kDefaultGeneric : precision == MGR_FP64 ? kDefaultStaged64 : kDefaultStaged;
     auto run = [&](auto pol) {
         using P = decltype(pol);
         auto go = [&](auto kern) {
