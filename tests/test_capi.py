@@ -58,7 +58,8 @@ def test_create_without_device_reports_cuda_error():
 def test_struct_layout_matches_header():
     """offsetof/sizeof of every struct field from gcc vs the ctypes mirror."""
     structs = {"mgr_model_desc": _capi.ModelDesc, "mgr_colpar_desc": _capi.ColparDesc,
-               "mgr_ali_opts": _capi.AliOpts}
+               "mgr_ali_opts": _capi.AliOpts, "mgr_mlp": _capi.MlpDesc,
+               "mgr_train_opts": _capi.TrainOpts, "mgr_tuning": _capi.Tuning}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} sizeof %zu\\n", sizeof({cname}));')
