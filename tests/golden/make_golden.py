@@ -21,6 +21,8 @@ CASES = {
     "lattice6": lambda: M.lattice_cloud(6, name="lattice6"),
     "wind6": lambda: M.wind_model(6, seed=21, nlev=5, nside=1, name="wind6"),
     "thick6": lambda: M.lattice_cloud(6, n_h2=1.0e15, name="thick6"),
+    # turbulent cloud: 41 bins per line, k^-4 velocity field (Doppler sub-points)
+    "turb6": lambda: M.turbulent_cloud(6, seed=31, nlev=6, npairs=6, nquads=41, name="turb6"),
 }
 
 
