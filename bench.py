@@ -223,7 +223,9 @@ class CpuOracle:
         self.nthreads = nthreads or os.cpu_count() or 1
         self.o = oracle.Oracle(model).setup()
 
-    def time(self, iterations, sample_s, seed=0):
+    def time(self, iterations, sample_s, seed=0, ng_steps=0):
+        """`iterations` formal solves (each with Jeff and the rate
+        equations) and `ng_steps` Ng steps."""
         import numpy as np
         m, o = self.model, self.o
         rng = np.random.default_rng(seed)
@@ -241,22 +243,53 @@ class CpuOracle:
         o.compute_Jeff()
         o.compute_level_populations_from_stateq()
         t_stateq = time.perf_counter() - t0
+        t_ng = 0.0
+        if ng_steps:
+            t0 = time.perf_counter()
+            o.ng_acceleration()
+            t_ng = time.perf_counter() - t0
         per_iter = t_solve + t_stateq
-        return {"seconds": per_iter * iterations, "per_iteration_s": per_iter,
-                "formal_solve_s": t_solve, "stateq_s": t_stateq,
+        return {"seconds": per_iter * iterations + t_ng * ng_steps, "per_iteration_s": per_iter,
+                "formal_solve_s": t_solve, "stateq_s": t_stateq, "ng_s": t_ng,
                 "sample_origins": int(len(origins)), "cores": self.nthreads}
 
 
 def cpu_oracle_time(model, iterations, sample_s, nthreads=None):
-    return CpuOracle(model, nthreads).time(iterations, sample_s)
+    """The oracle's time for `iterations` iterations of the ALI loop, Ng
+    steps (every fifth iteration) charged as Ng steps, not formal solves."""
+    from oracle.measure_iterations import step_kinds
+    k = step_kinds(iterations)
+    info = CpuOracle(model, nthreads).time(k.count("solve"), sample_s, ng_steps=k.count("ng"))
+    info["formal_solves"], info["ng_steps"] = k.count("solve"), k.count("ng")
+    return info
 
 
-# iterations of the FP64 solve of the default workload; the reference arm,
-# which cannot afford the full solve on CPU, multiplies its per-iteration
-# time by the count the same algorithm needs (equal iteration counts of
-# the oracle and the device path are checked by the GPU tests).
-REFERENCE_ITERATIONS = {"wind64": 5, "wind32": None, "lattice16": None, "batch256": None,
-                        "turb128": None}
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def reference_counts(name, model):
+    """(formal solves, Ng steps, source) of the reference's ALI (LTE start,
+    FP64) on this workload: from the record of a full oracle run
+    (oracle/measure_iterations.py), else -- for workloads small enough --
+    from running the oracle's ALI here."""
+    from oracle.measure_iterations import step_kinds
+    rec = os.path.join(ROOT, "oracle", f"iterations_{name}.json")
+    if os.path.exists(rec):
+        d = json.load(open(rec))
+        return d["formal_solves"], d["ng_steps"], f"measured full oracle ALI ({d['iterations']} iterations, oracle/iterations_{name}.json)"
+    if model.ncells <= 40 ** 3:
+        import oracle
+        it, _ = oracle.Oracle(model).setup().compute_level_populations(True, MAX_ITER, TOL)
+        k = step_kinds(it)
+        return k.count("solve"), k.count("ng"), f"oracle ALI run here ({it} iterations)"
+    return None, None, None
 
 
 def run_reference(args):
@@ -264,21 +297,18 @@ def run_reference(args):
     if rank != 0:
         return
     model = make_model(args.workload)
-    iters = REFERENCE_ITERATIONS.get(args.workload)
-    if iters is None:
-        import oracle
-        o = oracle.Oracle(model).setup() if args.workload == "lattice16" else None
-        if o is not None:
-            iters, _ = o.compute_level_populations(True, MAX_ITER, TOL)
-        else:
-            iters = REFERENCE_ITERATIONS["wind64"]
+    n_solve, n_ng, source = reference_counts(args.workload, model)
+    if n_solve is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"no measured iteration count of the oracle for {args.workload}"}))
+        return
     cpu = CpuOracle(model)
     for w in range(args.warmup):
-        cpu.time(iters, min(2.0, args.cpu_sample_s), seed=100 + w)
+        cpu.time(n_solve, min(2.0, args.cpu_sample_s), seed=100 + w, ng_steps=n_ng)
     steps = []
     info = None
     for k in range(max(1, args.steps)):
-        info = cpu.time(iters, args.cpu_sample_s, seed=k)
+        info = cpu.time(n_solve, args.cpu_sample_s, seed=k, ng_steps=n_ng)
         steps.append(info["seconds"])
     value = statistics.mean(steps)
     line = {
@@ -287,17 +317,64 @@ def run_reference(args):
         "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": workload_config(args.workload, model, "fp64"),
-        "ali_iterations": iters,
+        "ali_iterations": n_solve + n_ng, "formal_solves": n_solve, "ng_steps": n_ng,
+        "iteration_source": source,
         "cpu_baseline": {"value": value, "unit": "s", "cores": info["cores"], "kind": "port",
+                         "cpu_model": cpu_model(),
                          "sample": f"one formal solve over {info['sample_origins']} seeded origins "
                                    f"x all ray pairs scaled to {model.ncells} origins, plus one "
-                                   f"full rate-equation step, x {iters} iterations"},
+                                   f"full Jeff + rate-equation step, x {n_solve} formal solves; "
+                                   f"plus {n_ng} full Ng step(s)"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------------ GPU arm
+
+def _max_rel(a, b, mask=None):
+    import numpy as np
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r = np.abs(a - b) / np.abs(b)
+    r[a == b] = 0.0
+    if mask is not None:
+        r = r[mask]
+    return float(np.nanmax(r)) if r.size else 0.0
+
+
+def precision_errors(sim, model, pop_head, prec):
+    """The headline arm's error against the plain FP64 arm of the same run,
+    which sits on the simulation when this is called: (1) its converged
+    populations against the FP64-converged ones (max relative difference
+    over levels with n > 1e-10 n_tot; both stop at a max relative change
+    below the tolerance, so this includes the convergence tolerance), and
+    (2) with the FP64-converged populations fixed, J (when it fits), Jlin and
+    the ALO of one formal solve in the headline precision against one in FP64
+    (the precision error alone)."""
+    import numpy as np
+    pop64 = sim.population
+    mask = pop64 > 1e-10 * model.population_tot[:, None]
+    out = {"pop_max_rel": _max_rel(pop_head, pop64, mask),
+           "pop_note": "converged populations of the headline arm vs the plain FP64 arm "
+                       "(levels with n > 1e-10 n_tot)"}
+    if prec == "fp64":
+        return out
+    keep_J = model.ncells * model.nfreqs <= 200_000_000
+    sim.compute_radiation_field(prec, keep_J=keep_J)
+    J_m = sim.J if keep_J else None
+    Jlin_m, L_m = sim.Jlin, sim.Lambda
+    sim.compute_radiation_field("fp64", keep_J=keep_J)
+    if keep_J:
+        out["J_max_rel"] = _max_rel(J_m, sim.J)
+    out["Jlin_max_rel"] = _max_rel(Jlin_m, sim.Jlin)
+    out["lambda_max_rel"] = _max_rel(L_m, sim.Lambda)
+    out["J_note"] = (f"one {prec} formal solve vs one FP64 formal solve on the FP64-converged "
+                     f"populations, all cells" + ("" if keep_J else " (J per bin not kept at this size)"))
+    sim.compute_radiation_field(prec, keep_J=False)
+    return out
+
 
 def run_b200(args):
     import numpy as np
@@ -372,6 +449,7 @@ def run_b200(args):
         clk.mark_end()
     launches = (sim.launch_count() - launches0) // max(1, args.steps)
     converged = bool(getattr(sim, "converged", False))
+    pop_head = sim.population          # converged populations of the headline arm
     model_iters = None
     if model.meta.get("segments"):
         import numpy as np
@@ -405,6 +483,7 @@ def run_b200(args):
 
     # ---- the plain method: FP64 from the LTE start (north-star comparison)
     plain = None
+    errors = None
     if not args.no_plain:
         print(json.dumps({"progress": "headline step done", "seconds": times, "iterations": iters,
                           "converged": converged, "history": err_hist}), file=sys.stderr,
@@ -422,6 +501,8 @@ def run_b200(args):
                                          "max": int(mit.max()), "sum": int(mit.sum())}
         plain["iterations_ratio"] = it_p / max(1, iters[-1])
         plain["wallclock_ratio"] = t_p / max(1e-12, statistics.mean(times))
+        plain["wallclock_ratio_median"] = t_p / max(1e-12, statistics.median(times))
+        errors = precision_errors(sim, model, pop_head, prec)
     sim.close()
 
     # ---- multi-GPU: max over ranks
@@ -438,9 +519,9 @@ def run_b200(args):
     bpu = 44.0 if prec == "fp64" else 24.0
     avg_ms = statistics.mean(solve_ms)
     achieved = solve_upd[-1] * bpu / (avg_ms / 1e3) / 1e9
-    # DRAM bytes per update of the staged mixed kernel from one ncu capture
-    # of the 32^3 wind (profiles/formal_solve_staged_wind32.md), scaled to
-    # this launch by its update count (same bins per chunk, same ratio)
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per update of
+    # the staged mixed kernel from one ncu capture of a launch on the wind,
+    # scaled to this launch by its update count
     traffic = (solve_upd[-1] * STAGED_DRAM_BYTES_PER_UPDATE
                if prec == "mixed" and tuning and tuning.get("kernel") == "staged" else None)
     line = {
@@ -450,7 +531,10 @@ def run_b200(args):
         "dtype": "f64" if prec == "fp64" else "f32+f64",
         "data": "synthetic (seeded)",
         "config": workload_config(args.workload, model, prec, start_name),
+        "step_s": {"mean": statistics.mean(times), "median": statistics.median(times),
+                   "min": min(times), "max": max(times)},
         "ali_iterations": iters[-1], "converged": converged,
+        "errors_vs_fp64": errors,
         "model_iterations": model_iters,
         "solve_kernel": tuning,
         "plain_fp64_lte": plain,
@@ -473,9 +557,11 @@ def run_b200(args):
         info = cpu_oracle_time(model, iters[-1], args.cpu_sample_s)
         line["cpu_baseline"] = {
             "value": info["seconds"], "unit": "s", "cores": info["cores"], "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": f"one formal solve over {info['sample_origins']} seeded origins x all ray "
-                      f"pairs scaled to {model.ncells} origins, plus one full rate-equation "
-                      f"step, x {iters[-1]} iterations"}
+                      f"pairs scaled to {model.ncells} origins, plus one full Jeff + "
+                      f"rate-equation step, x {info['formal_solves']} formal solves, plus "
+                      f"{info['ng_steps']} full Ng step(s) ({iters[-1]} iterations)"}
     print(json.dumps(line), flush=True)
 
 

@@ -369,12 +369,18 @@ mgr_status mgr_get_tuning(mgr_handle *h, int32_t precision, mgr_tuning *out);
  *   stream     cudaStream_t to run on (NULL: the default stream)
  * Calls no allocator.  Its scratch is a fixed 1.5 MiB array inside the
  * library that every GPU loading the library holds until the process exits;
- * ncells*nlev above MGR_NOALLOC_MAX_ELEMENTS returns MGR_ERR_TOO_LARGE.  The
- * first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the array: calls
- * that overlap on the GPU (on different streams) race; nothing in it needs
- * clearing between calls.  Asynchronous: results are in `stats` once the
- * stream reaches that point. */
+ * ncells*nlev above MGR_NOALLOC_MAX_ELEMENTS returns MGR_ERR_TOO_LARGE.
+ * Every call on a stream that is not capturing looks up the array's device
+ * address in the current context (so a cudaDeviceReset between calls is
+ * harmless); a call on a capturing stream reuses the address that the last
+ * call outside capture found on this device, and returns MGR_ERR_STATE when
+ * there was none: make the first call on each device before any stream
+ * capture, and again after a cudaDeviceReset.  A CUDA error already pending
+ * on the calling thread from earlier work is reported as MGR_ERR_CUDA
+ * without launching anything and is left in place for the caller.  All
+ * calls share the array: calls that overlap on the GPU (on different
+ * streams) race; nothing in it needs clearing between calls.  Asynchronous:
+ * results are in `stats` once the stream reaches that point. */
 mgr_status mgr_convergence_noalloc(const double *pop, const double *prev, const double *pop_tot,
                                    int64_t ncells, int32_t nlev, double pop_prec, double *stats,
                                    void *stream);

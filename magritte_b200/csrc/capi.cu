@@ -86,8 +86,12 @@ struct mgr_handle {
     int64_t trace_budget = 0;
     double updates_per_solve = 0.0;
     int max_pair_points = 0;
-    std::vector<int32_t> h_len;        // [nrays*N] host copy for npoints
+    std::vector<int32_t> h_len;        // [nrays*N] host copy for npoints, made on demand
+    bool h_len_valid = false;
     std::vector<float> upd_origin;     // [N] updates of one formal solve per origin (batches)
+    unsigned long long *tstats_d = nullptr, *h_tstats = nullptr;   // trace statistics [3]
+    int32_t *pts_origin_d = nullptr;   // [N] points of each origin's traces
+    float *upd_origin_d = nullptr;     // [N] updates per origin (batches)
 
     bool model_loaded = false, line_set = false, bdy_set = false, pops_valid = false;
     bool keep_J = false;
@@ -202,6 +206,11 @@ void free_model(mgr_handle *h) {
     free_segments(h);
     free_traces(h);
     free_ptr((void *&)h->len_all);
+    free_ptr((void *&)h->tstats_d);
+    free_ptr((void *&)h->pts_origin_d);
+    free_ptr((void *&)h->upd_origin_d);
+    h->h_len.clear();
+    h->h_len_valid = false;
     for (void *p : h->model_allocs) cudaFree(p);
     h->model_allocs.clear();
     void **state[] = {(void **)&h->pop, (void **)&h->prev1, (void **)&h->prev2, (void **)&h->prev3,
@@ -548,47 +557,55 @@ int64_t default_budget(mgr_handle *h) {
     return (int64_t)(0.6 * (double)fr) + h->tcap * kBytesPerPoint;
 }
 
+// Host copy of the trace lengths (for get_npoints_on_rays and get_trace).
+void host_lens(mgr_handle *h) {
+    if (h->h_len_valid) return;
+    const int64_t n = (int64_t)h->nrays * h->N;
+    h->h_len.resize(n);
+    ck(cudaMemcpy(h->h_len.data(), h->len_all, n * sizeof(int32_t), cudaMemcpyDeviceToHost), "d2h lens");
+    h->h_len_valid = true;
+}
+
 void do_trace(mgr_handle *h) {
     need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
     set_device(h);
     // keep the point buffers of an earlier trace for reuse (freeing and
-    // allocating several GB costs more than the trace itself)
+    // allocating several GB costs more than the trace itself); captured
+    // graphs stay valid unless a buffer or the storage mode changes
+    const void *old_bufs[] = {h->tcell, h->tshift, h->tdz, h->tmp_, h->off_all};
+    const bool old_stored = h->stored;
     h->traced = false;
     h->stored = false;
-    h->gen++;
+    h->h_len_valid = false;
     const int old_max_pair = h->max_pair_points;
     const int64_t N = h->N, R = h->nrays, n = R * N;
-    h->max_pair_points = 0;
     if (!h->len_all) h->len_all = dalloc<int32_t>(h, n, nullptr);
+    if (!h->tstats_d) {
+        h->tstats_d = dalloc<unsigned long long>(h, 3, nullptr);
+        h->pts_origin_d = dalloc<int32_t>(h, N, nullptr);
+        if (!h->h_tstats) ck(cudaMallocHost(&h->h_tstats, 3 * sizeof(unsigned long long)), "pinned");
+    }
+    if (h->nseg > 0 && !h->upd_origin_d) h->upd_origin_d = dalloc<float>(h, N, nullptr);
     reset_flags(h);
     ck(launch_trace_count(h->mv, 0, N, h->len_all, h->flags, h->stream), "trace count");
-    h->launches += 1;
+    // ray-point-frequency updates of one formal solve, the longest pair and
+    // the points per origin, reduced on the device
+    ck(launch_trace_stats(h->mv, h->len_all, h->tstats_d, h->pts_origin_d,
+                          h->nseg > 0 ? h->upd_origin_d : nullptr, h->stream), "trace stats");
+    h->launches += 2;
+    ck(cudaMemcpyAsync(h->h_tstats, h->tstats_d, 3 * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, h->stream), "trace stats");
     check_flags(h, "trace");
-    h->h_len.resize(n);
-    ck(cudaMemcpy(h->h_len.data(), h->len_all, n * sizeof(int32_t), cudaMemcpyDeviceToHost), "d2h lens");
-    // ray-point-frequency updates of one formal solve
-    double U = 0.0;
-    int64_t total = 0;
-    std::vector<int64_t> per_origin(N, 0);
-    if (h->nseg > 0) h->upd_origin.assign(N, 0.0f);
-    else h->upd_origin.clear();
-    for (int64_t d = 0; d < R; d++)
-        for (int64_t o = 0; o < N; o++) {
-            total += h->h_len[d * N + o];
-            per_origin[o] += h->h_len[d * N + o];
-        }
-    for (int r = 0; r < h->npairs; r++) {
-        const int64_t ar = h->antipod[r];
-        for (int64_t o = 0; o < N; o++) {
-            const int64_t ndep = (int64_t)h->h_len[r * N + o] + h->h_len[ar * N + o] + 1;
-            if (ndep > 1) {
-                U += (double)ndep;
-                if (h->nseg > 0) h->upd_origin[o] += (float)(ndep * h->nfreqs);
-            }
-            h->max_pair_points = std::max<int>(h->max_pair_points, (int)(ndep - 1));
-        }
+    const int64_t total = (int64_t)h->h_tstats[0];
+    h->updates_per_solve = (double)h->h_tstats[1] * h->nfreqs;
+    h->max_pair_points = (int)h->h_tstats[2];
+    if (h->nseg > 0) {
+        h->upd_origin.resize(N);
+        ck(cudaMemcpy(h->upd_origin.data(), h->upd_origin_d, N * sizeof(float),
+                      cudaMemcpyDeviceToHost), "d2h updates");
+    } else {
+        h->upd_origin.clear();
     }
-    h->updates_per_solve = U * h->nfreqs;
     if (h->max_pair_points != old_max_pair) {   // tuned shapes depend on the ray lengths
         h->tune[0] = mgr_handle::Tune{};
         h->tune[1] = mgr_handle::Tune{};
@@ -609,6 +626,9 @@ void do_trace(mgr_handle *h) {
         h->batch_origins = N;
     } else {
         // origins per batch so that the largest batch fits the budget
+        std::vector<int32_t> per_origin(N);
+        ck(cudaMemcpy(per_origin.data(), h->pts_origin_d, N * sizeof(int32_t),
+                      cudaMemcpyDeviceToHost), "d2h points");
         const int64_t cap_pts = std::max<int64_t>(budget / kBytesPerPoint, 1);
         int64_t best = N;
         for (;;) {
@@ -624,6 +644,8 @@ void do_trace(mgr_handle *h) {
         h->batch_origins = best;
         h->stored = false;
     }
+    const void *new_bufs[] = {h->tcell, h->tshift, h->tdz, h->tmp_, h->off_all};
+    if (old_stored != h->stored || !std::equal(old_bufs, old_bufs + 5, new_bufs)) h->gen++;
     h->traced = true;
 }
 
@@ -991,6 +1013,7 @@ mgr_status mgr_destroy(mgr_handle *h) {
     if (h->h_stats) cudaFreeHost(h->h_stats);
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->h_patch) cudaFreeHost(h->h_patch);
+    if (h->h_tstats) cudaFreeHost(h->h_tstats);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->tev0) cudaEventDestroy(h->tev0);
@@ -1066,6 +1089,7 @@ mgr_status mgr_get_npoints_on_rays(mgr_handle *h, int64_t *npoints) {
     return run(h, [&] {
         need(npoints != nullptr, MGR_ERR_INVALID_ARG, "NULL output");
         if (!h->traced) do_trace(h);
+        host_lens(h);
         const int64_t N = h->N;
         for (int r = 0; r < h->npairs; r++) {
             const int64_t ar = h->antipod[r];
@@ -1083,6 +1107,7 @@ mgr_status mgr_get_trace(mgr_handle *h, int64_t o, int64_t r, int64_t cap, int64
         need(o >= 0 && o < h->N && r >= 0 && r < h->nrays, MGR_ERR_INVALID_ARG, "origin/ray out of range");
         set_device(h);
         if (!h->traced) do_trace(h);
+        host_lens(h);
         const int64_t len = h->h_len[r * h->N + o];
         *n = len;
         const int64_t m = std::min(len, cap);

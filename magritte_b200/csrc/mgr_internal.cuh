@@ -135,6 +135,11 @@ cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_co
 cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
                               double *shift, double *dZ, MixedPoint *mp, DevFlags *flags,
                               cudaStream_t s);
+// acc[0] = points of all traces, acc[1] = sum over (pair, origin) of ndep
+// where ndep > 1, acc[2] = the longest ray pair (points); pts_origin[N] and
+// upd_origin[N] (updates of one formal solve per origin) when not null.
+cudaError_t launch_trace_stats(const ModelView &m, const int32_t *len, unsigned long long *acc,
+                               int32_t *pts_origin, float *upd_origin, cudaStream_t s);
 
 struct SolveArgs {
     const double *eps, *kap;        // [N*K] emissivity, opacity (FP64 path)

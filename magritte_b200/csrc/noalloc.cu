@@ -100,20 +100,31 @@ __global__ void noalloc_final_kernel(const double *partials, int nblocks, double
     }
 }
 
-// Device address of the scratch array on the current device.  The first
-// call on a device looks it up (cudaGetSymbolAddress: the array's host-side
-// name is only a stand-in and must not be given to a kernel).
-cudaError_t partials_on_current_device(double **out) {
+// Device address of the scratch array on the current device.  The array's
+// host-side name is only a stand-in and must never be given to a kernel;
+// cudaGetSymbolAddress gives the address in the current context.  A call on
+// a stream that is not capturing looks the address up again (a host-side
+// table lookup, no allocation), so a cudaDeviceReset or a new primary
+// context between calls cannot leave a stale address behind.  A call on a
+// capturing stream uses the address that the last call outside capture
+// found on this device; with none yet it returns cudaErrorStreamCaptureUnsupported
+// without touching the runtime's module state inside the capture.
+cudaError_t partials_on_current_device(cudaStream_t s, double **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_dev[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_partials);
         if (e != cudaSuccess) return e;
         g_partials_dev[dev] = static_cast<double *>(p);
+    } else if (!g_partials_dev[dev]) {
+        return cudaErrorStreamCaptureUnsupported;
     }
     *out = g_partials_dev[dev];
     return cudaSuccess;
@@ -128,10 +139,15 @@ extern "C" mgr_status mgr_convergence_noalloc(const double *pop, const double *p
     if (!pop || !prev || !pop_tot || !stats || ncells <= 0 || nlev <= 0) return MGR_ERR_INVALID_ARG;
     if (ncells > MGR_NOALLOC_MAX_ELEMENTS / nlev) return MGR_ERR_TOO_LARGE;
     const int64_t n = ncells * (int64_t)nlev;
-    double *partials = nullptr;
-    if (partials_on_current_device(&partials) != cudaSuccess) return MGR_ERR_CUDA;
-    const int nblocks = (int)((n + kPerBlock - 1) / kPerBlock);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an error left pending on this host thread by earlier work is the
+    // caller's: report it without launching and leave it in place
+    if (cudaPeekAtLastError() != cudaSuccess) return MGR_ERR_CUDA;
+    double *partials = nullptr;
+    const cudaError_t e = partials_on_current_device(s, &partials);
+    if (e == cudaErrorStreamCaptureUnsupported) return MGR_ERR_STATE;
+    if (e != cudaSuccess) return MGR_ERR_CUDA;
+    const int nblocks = (int)((n + kPerBlock - 1) / kPerBlock);
     noalloc_partials_kernel<<<nblocks, kThreads, 0, s>>>(pop, prev, pop_tot, n, nlev, pop_prec,
                                                          partials);
     if (cudaGetLastError() != cudaSuccess) return MGR_ERR_CUDA;

@@ -196,7 +196,54 @@ __global__ void __launch_bounds__(128) trace_fill_kernel(ModelView m, TraceView 
     if (sink.over || (code == 0 && sink.n != sink.cap)) atomicAdd(&flags->cap_err, 1ull);
 }
 
+// Statistics of a counted trace, one thread per origin: the points of every
+// direction, the ray-point sum of the formal solve's update count
+// (sum over pairs of ndep = n_r + n_ar + 1 where ndep > 1, as
+// get_npoints_on_rays counts them, simulation.tpp:540-552), the longest ray
+// pair, and optionally each origin's points and updates.
+__global__ void __launch_bounds__(256) trace_stats_kernel(const int32_t *__restrict__ len,
+                                                          const int32_t *__restrict__ antipod,
+                                                          int64_t N, int R, int npairs, int nfreqs,
+                                                          unsigned long long *acc,
+                                                          int32_t *pts_origin, float *upd_origin) {
+    const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long pts = 0, U = 0, mx = 0;
+    if (o < N) {
+        for (int d = 0; d < R; d++) pts += (unsigned)len[(int64_t)d * N + o];
+        for (int r = 0; r < npairs; r++) {
+            const unsigned long long ndep =
+                (unsigned)len[(int64_t)r * N + o] + (unsigned)len[(int64_t)antipod[r] * N + o] + 1ull;
+            if (ndep > 1) U += ndep;
+            mx = ndep - 1 > mx ? ndep - 1 : mx;
+        }
+        if (pts_origin) pts_origin[o] = (int32_t)pts;
+        if (upd_origin) upd_origin[o] = (float)((double)U * nfreqs);
+    }
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+        pts += __shfl_xor_sync(0xffffffffu, pts, sh);
+        U += __shfl_xor_sync(0xffffffffu, U, sh);
+        const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, mx, sh);
+        mx = m2 > mx ? m2 : mx;
+    }
+    if ((threadIdx.x & 31) == 0 && (pts | U | mx)) {
+        atomicAdd(acc + 0, pts);
+        atomicAdd(acc + 1, U);
+        atomicMax(acc + 2, mx);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_trace_stats(const ModelView &m, const int32_t *len, unsigned long long *acc,
+                               int32_t *pts_origin, float *upd_origin, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(acc, 0, 3 * sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    const int64_t blocks = (m.N + 255) / 256;
+    trace_stats_kernel<<<(unsigned)blocks, 256, 0, s>>>(len, m.antipod, m.N, m.nrays, m.npairs,
+                                                        m.nfreqs, acc, pts_origin, upd_origin);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_count,
                                int32_t *len, DevFlags *flags, cudaStream_t s) {

@@ -12,7 +12,7 @@ forward, backward and Adam kernels (``mgr_mlp_train``).
     python -m magritte_b200.learned train --n 32 --models 12 --epochs 600 \
         --out magritte_b200/weights/wind_rotor10.npz
     python -m magritte_b200.learned train --family turb --n 64 --models 8 --nlev 21 \
-        --epochs 300 --subsample 0.25 --out magritte_b200/weights/turb_rotor21.npz
+        --epochs 600 --subsample 0.5 --out magritte_b200/weights/turb_rotor21.npz
 """
 from __future__ import annotations
 

@@ -1,0 +1,140 @@
+// ref_driver.cpp -- runs the reference's own C++ (Magritte's CPU path, built
+// from its unmodified sources by oracle/ref_build.sh into oracle/_ref) on a
+// model folder in Magritte's text layout, and writes what it computes as
+// raw little-endian arrays (TEST INFRASTRUCTURE ONLY: a second checker of
+// the C oracle, never part of the product).
+//
+//   magritte_ref <model/> <out/> radiation     J, Jlin, Jeff, ALO after one
+//                                              compute_radiation_field (LTE
+//                                              populations, or the model's
+//                                              population.txt with --pops)
+//   magritte_ref <model/> <out/> ali <n>       compute_level_populations(io,
+//                                              Ng, n): populations, the
+//                                              max and mean relative change
+//                                              of every iteration
+//   magritte_ref <model/> <out/> trace <o...>  the traced points of every
+//                                              ray of the given origins
+//
+// The call sequence follows the reference's examples
+// (src/examples/example_1.cpp: read, compute_spectral_discretisation,
+// compute_boundary_intensities, compute_LTE_level_populations, ...), with
+// the boundary temperatures of the model folder passed to
+// compute_boundary_intensities (sim_radiation.tpp:17-40).
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "Io/cpp/io_cpp_text.hpp"
+#include "Simulation/simulation.hpp"
+
+namespace {
+
+void write_raw(const std::string &path, const std::vector<double> &v) {
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char *>(v.data()), (std::streamsize)(v.size() * sizeof(double)));
+}
+
+void write_raw_long(const std::string &path, const std::vector<long> &v) {
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char *>(v.data()), (std::streamsize)(v.size() * sizeof(long)));
+}
+
+void set_up(Simulation &sim, bool lte) {
+    sim.compute_spectral_discretisation();
+    sim.compute_boundary_intensities(sim.geometry.boundary.boundary_temperature);
+    if (lte) {
+        sim.compute_LTE_level_populations();
+    } else {
+        // populations read from the model folder (Model::read)
+        sim.lines.set_emissivity_and_opacity();
+    }
+}
+
+// Jlin[p][k] and the diagonal ALO element of (p, k) (sum of the elements
+// whose position is p itself; with n_off_diag = 0 there is one).
+void write_line_fields(Simulation &sim, const std::string &out) {
+    const LineProducingSpecies &ls = sim.lines.lineProducingSpecies[0];
+    const size_t N = sim.parameters.ncells(), K = ls.linedata.nrad;
+    std::vector<double> jl(N * K), je(N * K), lam(N * K, 0.0);
+    for (size_t p = 0; p < N; p++)
+        for (size_t k = 0; k < K; k++) {
+            jl[p * K + k] = ls.Jlin[p][k];
+            je[p * K + k] = ls.Jeff[p][k];
+            for (size_t i = 0; i < ls.lambda.Ls[p][k].size(); i++)
+                if ((size_t)ls.lambda.nr[p][k][i] == p) lam[p * K + k] += ls.lambda.Ls[p][k][i];
+        }
+    write_raw(out + "/Jlin.bin", jl);
+    write_raw(out + "/Jeff.bin", je);
+    write_raw(out + "/Lambda.bin", lam);
+}
+
+void write_populations(Simulation &sim, const std::string &out) {
+    const LineProducingSpecies &ls = sim.lines.lineProducingSpecies[0];
+    std::vector<double> pop(ls.population.size());
+    for (size_t i = 0; i < pop.size(); i++) pop[i] = ls.population[i];
+    write_raw(out + "/population.bin", pop);
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    if (argc < 4) {
+        std::fprintf(stderr, "usage: %s <model/> <out/> radiation [--pops] | ali <n> | trace <o>...\n",
+                     argv[0]);
+        return 2;
+    }
+    const std::string model = argv[1], out = argv[2], cmd = argv[3];
+    IoText io(model);
+    Simulation sim;
+    sim.read(io);
+    if (cmd == "radiation") {
+        const bool lte = !(argc > 4 && std::string(argv[4]) == "--pops");
+        set_up(sim, lte);
+        sim.compute_radiation_field();
+        sim.compute_Jeff();
+        std::vector<double> J(sim.radiation.J.size());
+        for (size_t i = 0; i < J.size(); i++) J[i] = sim.radiation.J[i];
+        write_raw(out + "/J.bin", J);
+        write_line_fields(sim, out);
+        write_populations(sim, out);
+        return 0;
+    }
+    if (cmd == "ali" && argc > 4) {
+        set_up(sim, true);
+        IoText io_out(out + "/");
+        const long it = sim.compute_level_populations(io_out, true, std::atol(argv[4]));
+        write_populations(sim, out);
+        write_raw(out + "/error_max.bin", sim.error_max);
+        write_raw(out + "/error_mean.bin", sim.error_mean);
+        write_raw_long(out + "/iterations.bin", std::vector<long>{it});
+        return 0;
+    }
+    if (cmd == "trace") {
+        sim.compute_spectral_discretisation();
+        std::vector<long> head;
+        std::vector<long> cells;
+        std::vector<double> sh, dz;
+        for (int a = 4; a < argc; a++) {
+            const long o = std::atol(argv[a]);
+            const double dsm = sim.get_dshift_max(o);
+            for (size_t r = 0; r < sim.parameters.nrays(); r++) {
+                const RayData rd = sim.geometry.trace_ray<CoMoving>(o, r, dsm);
+                head.push_back((long)rd.size());
+                for (const ProjectedCellData &d : rd) {
+                    cells.push_back(d.cellNr);
+                    sh.push_back(d.shift);
+                    dz.push_back(d.dZ);
+                }
+            }
+        }
+        write_raw_long(out + "/trace_len.bin", head);
+        write_raw_long(out + "/trace_cell.bin", cells);
+        write_raw(out + "/trace_shift.bin", sh);
+        write_raw(out + "/trace_dZ.bin", dz);
+        return 0;
+    }
+    std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
+    return 2;
+}

@@ -61,3 +61,50 @@ def test_convergence_noalloc_rejects_oversize(gpu):
     assert st == 10   # MGR_ERR_TOO_LARGE
     st = lib.mgr_convergence_noalloc(None, fake, fake, 10, 2, 1e-6, fake, None)
     assert st == 1    # MGR_ERR_INVALID_ARG
+
+
+def _numpy_convergence(pop, prev, tot, nlev, pop_prec):
+    """check_for_convergence (lineProducingSpecies.tpp:120-171) restated in
+    numpy: count, mean and max of 2|n - n'|/(n + n') over levels with
+    n > 1e-10 n_tot."""
+    a = pop.reshape(-1)
+    b = prev.reshape(-1)
+    keep = a > 1.0e-10 * np.repeat(tot, nlev)
+    rc = 2.0 * np.abs(a - b)
+    rc = rc / (a + b)
+    rc = np.where(keep, rc, 0.0)
+    n = a.size
+    return float(np.count_nonzero(rc > pop_prec)) / n, float(rc.sum()) / n, float(rc.max())
+
+
+@pytest.mark.parametrize("ncells,nlev", [(400_000, 3), (16_777_216, 4)])
+def test_convergence_noalloc_large(gpu, ncells, nlev):
+    """More than 1024 first-pass blocks (the final pass loops over the
+    partials), and exactly MGR_NOALLOC_MAX_ELEMENTS cell-levels (65,536
+    blocks, the whole scratch array), on synthetic device arrays."""
+    import torch
+    assert ncells * nlev > 1_048_576
+    rng = np.random.default_rng(ncells)
+    prev = rng.lognormal(0.0, 3.0, size=(ncells, nlev))
+    pop = prev * (1.0 + rng.normal(0.0, 1e-3, size=prev.shape))
+    pop[rng.random(size=pop.shape) < 1e-3] *= 1e-12      # below 1e-10 n_tot: skipped
+    tot = pop.sum(axis=1)
+    ref = _numpy_convergence(pop, prev, tot, nlev, 1e-4)
+    dev = torch.device("cuda", 0)
+    tp = torch.from_numpy(pop).to(dev)
+    tq = torch.from_numpy(prev).to(dev)
+    tt = torch.from_numpy(tot).to(dev)
+    stats = torch.empty(3, dtype=torch.float64, device=dev)
+    lib = _capi.load()
+    for _ in range(2):
+        stats.fill_(float("nan"))
+        st = lib.mgr_convergence_noalloc(tp.data_ptr(), tq.data_ptr(), tt.data_ptr(), ncells,
+                                         nlev, 1e-4, stats.data_ptr(), None)
+        assert st == 0
+        torch.cuda.synchronize()
+        got = stats.cpu().numpy()
+        assert got[0] == pytest.approx(ref[0], rel=1e-12, abs=0.0)
+        assert got[1] == pytest.approx(ref[1], rel=1e-11)
+        assert got[2] == ref[2]
+    del tp, tq, tt
+    torch.cuda.empty_cache()
