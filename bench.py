@@ -25,9 +25,13 @@ solve from LTE is measured in the same run and reported beside it.
 restated in C, OpenMP over origins as the reference does) the same way and
 prints one line with "impl": "reference".
 
-Multi-GPU (torchrun): every rank solves its own replica (no exchange on
-the data path); value is the job's max time over ranks divided by the
-number of solves.
+Multi-GPU (torchrun): the ranks partition the origins of the one model
+(``magritte_b200.partition``: each rank solves its own origins and cells,
+then one NCCL all-gather of the population blocks per iteration), so the
+scaling is strong and value is the max over ranks of the time per
+converged solve.  ``--replicas`` solves an independent replica per GPU
+instead (weak scaling); ``--partition`` runs the partitioned driver on one
+GPU.
 """
 from __future__ import annotations
 
@@ -71,6 +75,12 @@ def parse():
     ap.add_argument("--plain-max-iter", type=int, default=None,
                     help="iteration cap of the plain FP64 solve (default: --max-iter); a plain "
                          "solve stopped by the cap reports converged: false and a lower bound")
+    ap.add_argument("--partition", action="store_true",
+                    help="run the partitioned driver (one shard per rank, NCCL all-gather of "
+                         "the populations every iteration) even on one GPU")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with several GPUs, solve an independent replica per GPU instead of "
+                         "partitioning one model")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -126,6 +136,15 @@ def max_over_ranks(values):
     t = torch.tensor(list(values), dtype=torch.float64, device=dev)
     tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
     return [float(x) for x in t.cpu()]
+
+
+def free_port():
+    import socket
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
 
 
 def dist_env():
@@ -381,12 +400,18 @@ def run_b200(args):
     from magritte_b200 import Simulation
     rank, world, local = dist_env()
     dist = world > 1
-    if dist:
+    partitioned = (dist and not args.replicas) or args.partition
+    if dist or partitioned:
         import datetime
         import torch
         import torch.distributed as tdist
         torch.cuda.set_device(local)
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if dist:
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        else:
+            tdist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{free_port()}",
+                                     rank=0, world_size=1,
+                                     timeout=datetime.timedelta(seconds=600))
     model = make_model(args.workload)
     prec = args.precision
     net = None
@@ -407,11 +432,23 @@ def run_b200(args):
         else:
             sim.compute_LTE_level_populations()
 
+    shards = {}
+
     def one_solve(sim, learned=net is not None, precision=prec, max_iter=None):
         sim.trace()
         start(sim, learned)
-        return sim.compute_level_populations(True, max_iter or args.max_iter, precision,
-                                             tol_max_rel=TOL, use_graph=graph)
+        if not partitioned:
+            return sim.compute_level_populations(True, max_iter or args.max_iter, precision,
+                                                 tol_max_rel=TOL, use_graph=graph)
+        # this rank's shard of the origins; one all-gather per iteration
+        from magritte_b200.partition import DeviceShard, partitioned_level_populations
+        key = (id(sim), precision)
+        if key not in shards:
+            shards[key] = DeviceShard(sim, rank, world, precision)
+        it, hist, conv = partitioned_level_populations(shards[key], None, True,
+                                                       max_iter or args.max_iter, TOL)
+        sim.error_max, sim.converged = hist, conv
+        return it
 
     # ---- device-resident solve
     sim = Simulation(model, device=local if dist else 0)
@@ -421,7 +458,7 @@ def run_b200(args):
     sim.compute_boundary_intensities()
     for _ in range(max(0, args.warmup - 1)):
         one_solve(sim)
-    if not args.no_plain and not args.no_autotune:
+    if not args.no_plain and not dist and not args.no_autotune:
         # tune the FP64 kernel before the plain solve is timed
         sim.trace()
         start(sim, False)
@@ -474,7 +511,13 @@ def run_b200(args):
         start(s2, net is not None)
         if not args.no_autotune:
             s2.set_autotune(True)
-        s2.compute_level_populations(True, args.max_iter, prec, tol_max_rel=TOL, use_graph=graph)
+        if partitioned:
+            from magritte_b200.partition import DeviceShard, partitioned_level_populations
+            partitioned_level_populations(DeviceShard(s2, rank, world, prec), None, True,
+                                          args.max_iter, TOL)
+        else:
+            s2.compute_level_populations(True, args.max_iter, prec, tol_max_rel=TOL,
+                                         use_graph=graph)
         pop = s2.population
         e2e.append(time.perf_counter() - t0)
         s2.close()
@@ -484,7 +527,7 @@ def run_b200(args):
     # ---- the plain method: FP64 from the LTE start (north-star comparison)
     plain = None
     errors = None
-    if not args.no_plain:
+    if not args.no_plain and not dist:
         print(json.dumps({"progress": "headline step done", "seconds": times, "iterations": iters,
                           "converged": converged, "history": err_hist}), file=sys.stderr,
               flush=True)
@@ -509,9 +552,10 @@ def run_b200(args):
     if dist:
         t_step, e2e_t = max_over_ranks([t_step, statistics.mean(e2e) if e2e else 0.0])
         tdist.barrier()
-        tdist.destroy_process_group()
     else:
         e2e_t = statistics.mean(e2e) if e2e else None
+    if dist or partitioned:
+        tdist.destroy_process_group()
     if rank != 0:
         return
 
@@ -525,12 +569,17 @@ def run_b200(args):
     traffic = (solve_upd[-1] * STAGED_DRAM_BYTES_PER_UPDATE
                if prec == "mixed" and tuning and tuning.get("kernel") == "staged" else None)
     line = {
-        "metric": METRIC, "value": t_step / world, "unit": "s", "n_gpus": world,
+        "metric": METRIC, "value": t_step if partitioned else t_step / world, "unit": "s",
+        "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": False, "scaling": "strong" if partitioned else "weak",
+        "vs_baseline": None,
         "dtype": "f64" if prec == "fp64" else "f32+f64",
         "data": "synthetic (seeded)",
-        "config": workload_config(args.workload, model, prec, start_name),
+        "config": dict(workload_config(args.workload, model, prec, start_name),
+                       parallelism=(f"origins partitioned over {world} GPU(s), populations "
+                                    f"all-gathered over NCCL every iteration" if partitioned
+                                    else ("one replica per GPU" if dist else "1 GPU"))),
         "step_s": {"mean": statistics.mean(times), "median": statistics.median(times),
                    "min": min(times), "max": max(times)},
         "ali_iterations": iters[-1], "converged": converged,
@@ -548,7 +597,8 @@ def run_b200(args):
                              f"staged kernel reads each point once per 32 bins: DRAM traffic is "
                              f"`traffic` bytes per launch, and the kernel is bound by instruction "
                              f"issue and the XU pipe, not HBM"},
-        "e2e": None if not e2e else {"value": e2e_t / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
+        "e2e": None if not e2e else {"value": e2e_t if partitioned else e2e_t / world, "unit": "s",
+                "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),

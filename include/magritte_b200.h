@@ -218,6 +218,19 @@ mgr_status mgr_get_Jlin(mgr_handle *h, double *Jlin);                 /* [ncells
 mgr_status mgr_get_Jeff(mgr_handle *h, double *Jeff);                 /* [ncells*nrad] */
 mgr_status mgr_get_lambda(mgr_handle *h, double *Ls);                 /* [ncells*nrad] */
 mgr_status mgr_get_emissivity_opacity(mgr_handle *h, double *eta, double *chi); /* [ncells*nrad] */
+
+/* The three previous iterates that Ng acceleration reads ([ncells*nlev]
+ * each; NULL skips one): with the populations they are what
+ * LineProducingSpecies::write stores (population, population_prev1..3,
+ * Model/Lines/LineProducingSpecies/lineProducingSpecies.cpp:105-135), so a
+ * run can be checkpointed and resumed exactly. */
+mgr_status mgr_get_population_history(mgr_handle *h, double *prev1, double *prev2, double *prev3);
+
+/* Restores populations and their history (a NULL previous iterate is set
+ * to zero, as the reference leaves it when the file is absent,
+ * lineProducingSpecies.cpp:60-95), then the emissivities and opacities. */
+mgr_status mgr_set_population_history(mgr_handle *h, const double *pop, const double *prev1,
+                                      const double *prev2, const double *prev3);
 mgr_status mgr_get_frequencies(mgr_handle *h, double *nu);            /* [ncells*nfreqs] */
 
 /* Device time of the last formal solve (ms, CUDA events on the handle's
@@ -307,6 +320,52 @@ mgr_status mgr_mlp_loss_grad(int device, const mgr_mlp *net, const float *X, con
                              const float *target, int64_t n, float *loss, float *grad);
 
 /* --- without allocation ------------------------------------------------- */
+
+/* --- partitioned runs (one shard per GPU) -------------------------------- */
+
+/* Restricts the handle to the origins [o_begin, o_end) of its model: the
+ * formal solve computes Jlin and the ALO of those origins only, and the
+ * statistical equilibrium updates those cells only.  Every shard keeps the
+ * whole model and the whole population history; after each rate-equation
+ * step the shards exchange the populations of their cells and their
+ * convergence partials (an all-gather over the shards), after which every
+ * shard holds the same arrays as an unpartitioned run and the Ng step and
+ * the emissivity update run on each shard alike.  Bounds must be multiples
+ * of 4 (or ncells).  Replaces the reference's split of the ray directions
+ * over MPI ranks with its reduction of J and gather of the ALO
+ * (Simulation/sim_radiation.tpp:130, Model/Radiation/radiation.cpp:292-325,
+ * Model/Lines/LineProducingSpecies/Lambda/lambda.tpp:191-317): partitioning
+ * by origin leaves each cell's J, ALO and rate equations on one shard, so no
+ * reduction of J is needed.  Not for batches of models. */
+mgr_status mgr_set_origin_range(mgr_handle *h, int64_t o_begin, int64_t o_end);
+
+/* Jeff and the statistical equilibrium of the shard's cells (the history
+ * of the other cells shifts as well); their convergence partials are left
+ * in MGR_BUF_CONVERGENCE_PARTIALS at the positions of their 4-cell blocks.
+ * The local half of Simulation::compute_level_populations_from_stateq
+ * (sim_lines.tpp:24-30) for a shard. */
+mgr_status mgr_stateq_local(mgr_handle *h);
+
+/* After the exchange: emissivities and opacities of every cell from the
+ * populations, and the convergence statistics from every block's partials
+ * (read them with mgr_get_convergence). */
+mgr_status mgr_stateq_finish(mgr_handle *h);
+
+typedef enum {
+    MGR_BUF_POPULATION = 0,            /* double [ncells*nlev] */
+    MGR_BUF_PREV1 = 1,                 /* double [ncells*nlev] */
+    MGR_BUF_PREV2 = 2,                 /* double [ncells*nlev] */
+    MGR_BUF_PREV3 = 3,                 /* double [ncells*nlev] */
+    MGR_BUF_JLIN = 4,                  /* double [ncells*nrad] */
+    MGR_BUF_LAMBDA = 5,                /* double [ncells*nrad] */
+    MGR_BUF_CONVERGENCE_PARTIALS = 6   /* double [3*ceil(ncells/4)]: count, sum, max per 4 cells */
+} mgr_buffer;
+
+/* Device address and element count of one of the handle's state arrays,
+ * for collectives that read and write them in place (an all-gather over
+ * NCCL).  The address stays valid until mgr_upload_model or mgr_destroy.
+ * No reference counterpart. */
+mgr_status mgr_get_device_buffer(mgr_handle *h, int32_t which, void **ptr, int64_t *count);
 
 /* --- batches of independent models ------------------------------------- */
 

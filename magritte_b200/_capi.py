@@ -38,8 +38,12 @@ EXPORTS = (
     "mgr_convergence_noalloc", "mgr_mlp_param_count", "mgr_get_features", "mgr_get_lte_logfrac",
     "mgr_warm_start", "mgr_mlp_train", "mgr_mlp_forward", "mgr_mlp_loss_grad",
     "mgr_set_segments", "mgr_get_segment_results", "mgr_set_autotune", "mgr_get_tuning",
-    "mgr_get_patch_stats",
+    "mgr_get_patch_stats", "mgr_set_origin_range", "mgr_stateq_local", "mgr_stateq_finish",
+    "mgr_get_device_buffer", "mgr_get_population_history", "mgr_set_population_history",
 )
+# mgr_buffer
+BUF_POPULATION, BUF_PREV1, BUF_PREV2, BUF_PREV3, BUF_JLIN, BUF_LAMBDA, BUF_PARTIALS = range(7)
+CELLS_PER_PARTIAL = 4
 MLP_FEATURES = 10
 MLP_HIDDEN = 128
 NOALLOC_MAX_ELEMENTS = 67108864
@@ -138,6 +142,12 @@ def load(build_if_missing: bool = True):
     L.mgr_get_emissivity_opacity.argtypes = [_P, _P, _P]
     L.mgr_get_solve_stats.argtypes = [_P, C.POINTER(_dbl), C.POINTER(_dbl)]
     L.mgr_convergence_noalloc.argtypes = [_P, _P, _P, _i64, _i32, _dbl, _P, _P]
+    L.mgr_set_origin_range.argtypes = [_P, _i64, _i64]
+    L.mgr_stateq_local.argtypes = [_P]
+    L.mgr_stateq_finish.argtypes = [_P]
+    L.mgr_get_device_buffer.argtypes = [_P, _i32, C.POINTER(_P), C.POINTER(_i64)]
+    L.mgr_get_population_history.argtypes = [_P, _P, _P, _P]
+    L.mgr_set_population_history.argtypes = [_P, _P, _P, _P, _P]
     L.mgr_mlp_param_count.argtypes = [_i32, C.POINTER(_i64)]
     L.mgr_get_features.argtypes = [_P, _P]
     L.mgr_get_lte_logfrac.argtypes = [_P, _P]

@@ -108,6 +108,16 @@ struct mgr_handle {
     int64_t last_patched = 0;
     int64_t fp64_fallbacks = 0;        // mixed solves redone in double (patch list full)
 
+    // warm start: features, LTE log fractions, network output and the
+    // network's parameters, kept between calls (allocated once per model)
+    float *ws_F = nullptr, *ws_L = nullptr, *ws_D = nullptr, *ws_P = nullptr;
+    float *ws_mean = nullptr, *ws_istd = nullptr;
+    int64_t ws_np = 0;
+
+    // origins (= cells) this handle solves: a shard of a partitioned run
+    int64_t o_begin = 0, o_end = 0;
+    bool whole() const { return o_begin == 0 && o_end == N; }
+
     // batch of independent models (nseg > 0)
     int64_t nseg = 0;
     int64_t *seg_begin_d = nullptr;
@@ -213,6 +223,10 @@ void free_model(mgr_handle *h) {
     h->h_len_valid = false;
     for (void *p : h->model_allocs) cudaFree(p);
     h->model_allocs.clear();
+    void **ws[] = {(void **)&h->ws_F, (void **)&h->ws_L, (void **)&h->ws_D, (void **)&h->ws_P,
+                   (void **)&h->ws_mean, (void **)&h->ws_istd};
+    for (void **p : ws) free_ptr(*p);
+    h->ws_np = 0;
     void **state[] = {(void **)&h->pop, (void **)&h->prev1, (void **)&h->prev2, (void **)&h->prev3,
                       (void **)&h->eps, (void **)&h->kap, (void **)&h->Jlin, (void **)&h->Lam,
                       (void **)&h->Jeff, (void **)&h->J, (void **)&h->partials, (void **)&h->stats,
@@ -259,6 +273,8 @@ LevelArgs level_args(mgr_handle *h) {
     a.Jlin = h->Jlin; a.Lam = h->Lam; a.Jeff = h->Jeff;
     a.partials = h->partials; a.stats = h->stats;
     a.npartials = level_partials_needed(h->mv);
+    a.c_begin = h->o_begin;
+    a.c_end = h->o_end;
     return a;
 }
 
@@ -297,6 +313,8 @@ void do_upload(mgr_handle *h, const mgr_model_desc *d) {
     set_device(h);
     const int64_t N = d->ncells;
     h->N = N;
+    h->o_begin = 0;
+    h->o_end = N;
     h->nrays = (int)d->nrays;
     h->npairs = (int)(d->nrays / 2);
     h->nlev = d->nlev;
@@ -591,7 +609,8 @@ void do_trace(mgr_handle *h) {
     // ray-point-frequency updates of one formal solve, the longest pair and
     // the points per origin, reduced on the device
     ck(launch_trace_stats(h->mv, h->len_all, h->tstats_d, h->pts_origin_d,
-                          h->nseg > 0 ? h->upd_origin_d : nullptr, h->stream), "trace stats");
+                          h->nseg > 0 ? h->upd_origin_d : nullptr, h->o_begin, h->o_end, h->stream),
+       "trace stats");
     h->launches += 2;
     ck(cudaMemcpyAsync(h->h_tstats, h->tstats_d, 3 * sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, h->stream), "trace stats");
@@ -696,6 +715,8 @@ SolveArgs solve_args(mgr_handle *h) {
     a.patch = h->patch;
     a.patch_count = h->patch_count;
     a.patch_cap = h->patch_cap;
+    a.s_begin = h->o_begin;   // origins of the stored trace (index = origin)
+    a.s_end = h->o_end;
     return a;
 }
 
@@ -861,13 +882,16 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
     reset_flags(h);
     unsigned long long patched = 0;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
-    for (int64_t o0 = 0; o0 < h->N; o0 += h->batch_origins) {
-        const int64_t cnt = std::min(h->batch_origins, h->N - o0);
+    for (int64_t o0 = h->o_begin; o0 < h->o_end; o0 += h->batch_origins) {
+        const int64_t cnt = std::min(h->batch_origins, h->o_end - o0);
         TraceView t = build_batch(h, o0, cnt);
+        SolveArgs ab = a;   // a batch's store holds exactly the origins it solves
+        ab.s_begin = 0;
+        ab.s_end = cnt;
         if (precision == MGR_MIXED)
             ck(cudaMemsetAsync(h->patch_count, 0, sizeof(unsigned long long), h->stream), "patch reset");
         int kind = 0;
-        ck(launch_formal_solve(h->mv, t, a, precision, variant, h->flags, h->stream, &kind),
+        ck(launch_formal_solve(h->mv, t, ab, precision, variant, h->flags, h->stream, &kind),
            "formal solve");
         h->tune[precision == MGR_MIXED].kind = kind;
         h->launches += precision == MGR_MIXED ? 2 : 1;
@@ -1151,7 +1175,71 @@ mgr_status mgr_compute_Jeff(mgr_handle *h) {
 }
 
 mgr_status mgr_compute_level_populations_from_stateq(mgr_handle *h) {
-    return run(h, [&] { do_stateq(h); });
+    return run(h, [&] {
+        need(h->whole(), MGR_ERR_STATE,
+             "a shard (origin range) updates its cells with mgr_stateq_local and mgr_stateq_finish");
+        do_stateq(h);
+    });
+}
+
+mgr_status mgr_set_origin_range(mgr_handle *h, int64_t o_begin, int64_t o_end) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        need(h->nseg == 0, MGR_ERR_UNSUPPORTED, "a batch of models is not partitioned");
+        need(0 <= o_begin && o_begin < o_end && o_end <= h->N, MGR_ERR_INVALID_ARG,
+             "origin range outside [0, ncells)");
+        need(o_begin % kCellsPerPartial == 0 && (o_end % kCellsPerPartial == 0 || o_end == h->N),
+             MGR_ERR_INVALID_ARG, "origin range bounds must be multiples of 4 (or ncells)");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        h->o_begin = o_begin;
+        h->o_end = o_end;
+        h->traced = false;   // the next trace counts the updates of this range
+        h->gen++;
+    });
+}
+
+mgr_status mgr_stateq_local(mgr_handle *h) {
+    return run(h, [&] {
+        need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+        set_device(h);
+        const LevelArgs a = level_args(h);
+        reset_flags(h);
+        ck(launch_jeff(h->mv, a, h->stream), "jeff");
+        ck(launch_stateq(h->mv, a, h->flags, h->stream), "stateq");
+        h->launches += 3;
+        check_flags(h, "statistical equilibrium");
+    });
+}
+
+mgr_status mgr_stateq_finish(mgr_handle *h) {
+    return run(h, [&] {
+        set_device(h);
+        const LevelArgs a = level_args(h);
+        ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
+        ck(launch_convergence_final(h->mv, a, h->stream), "convergence");
+        h->launches += 2;
+        read_stats(h);
+    });
+}
+
+mgr_status mgr_get_device_buffer(mgr_handle *h, int32_t which, void **ptr, int64_t *count) {
+    return run(h, [&] {
+        need(h->model_loaded && ptr && count, MGR_ERR_INVALID_ARG, "no model or NULL output");
+        switch (which) {
+            case MGR_BUF_POPULATION: *ptr = h->pop; *count = h->N * h->nlev; break;
+            case MGR_BUF_PREV1: *ptr = h->prev1; *count = h->N * h->nlev; break;
+            case MGR_BUF_PREV2: *ptr = h->prev2; *count = h->N * h->nlev; break;
+            case MGR_BUF_PREV3: *ptr = h->prev3; *count = h->N * h->nlev; break;
+            case MGR_BUF_JLIN: *ptr = h->Jlin; *count = h->N * h->nrad; break;
+            case MGR_BUF_LAMBDA: *ptr = h->Lam; *count = h->N * h->nrad; break;
+            case MGR_BUF_CONVERGENCE_PARTIALS:
+                *ptr = h->partials;
+                *count = 3 * ((h->N + kCellsPerPartial - 1) / kCellsPerPartial);
+                break;
+            default: fail(MGR_ERR_INVALID_ARG, "unknown buffer");
+        }
+    });
 }
 
 mgr_status mgr_ng_acceleration(mgr_handle *h) {
@@ -1175,6 +1263,8 @@ mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts
         need(opts->max_iter >= 1, MGR_ERR_INVALID_ARG, "max_iter must be >= 1");
         need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
         need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+        need(h->whole(), MGR_ERR_STATE,
+             "a shard (origin range) iterates through a partitioned driver, not this loop");
         const bool graph = opts->use_graph != 0;
         auto converged = [&](double fnc, double mx) {
             return opts->tol_max_rel > 0.0 ? mx < opts->tol_max_rel : !(fnc > 0.005);
@@ -1343,6 +1433,39 @@ MGR_GETTER(mgr_get_Jlin, h->Jlin, h->N * h->nrad)
 MGR_GETTER(mgr_get_Jeff, h->Jeff, h->N * h->nrad)
 MGR_GETTER(mgr_get_lambda, h->Lam, h->N * h->nrad)
 
+mgr_status mgr_get_population_history(mgr_handle *h, double *prev1, double *prev2, double *prev3) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_INVALID_ARG, "no model uploaded");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        const size_t bytes = (size_t)h->N * h->nlev * sizeof(double);
+        if (prev1) ck(cudaMemcpy(prev1, h->prev1, bytes, cudaMemcpyDeviceToHost), "d2h");
+        if (prev2) ck(cudaMemcpy(prev2, h->prev2, bytes, cudaMemcpyDeviceToHost), "d2h");
+        if (prev3) ck(cudaMemcpy(prev3, h->prev3, bytes, cudaMemcpyDeviceToHost), "d2h");
+    });
+}
+
+mgr_status mgr_set_population_history(mgr_handle *h, const double *pop, const double *prev1,
+                                      const double *prev2, const double *prev3) {
+    return run(h, [&] {
+        need(h->model_loaded && pop, MGR_ERR_INVALID_ARG, "no model or NULL populations");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        const size_t bytes = (size_t)h->N * h->nlev * sizeof(double);
+        ck(cudaMemcpy(h->pop, pop, bytes, cudaMemcpyHostToDevice), "h2d");
+        double *dst[3] = {h->prev1, h->prev2, h->prev3};
+        const double *src[3] = {prev1, prev2, prev3};
+        for (int i = 0; i < 3; i++) {
+            if (src[i]) ck(cudaMemcpy(dst[i], src[i], bytes, cudaMemcpyHostToDevice), "h2d");
+            else ck(cudaMemset(dst[i], 0, bytes), "memset");
+        }
+        ck(launch_emissivity_opacity(h->mv, level_args(h), h->stream), "emissivity");
+        h->launches += 1;
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        h->pops_valid = true;
+    });
+}
+
 mgr_status mgr_get_emissivity_opacity(mgr_handle *h, double *eta, double *chi) {
     return run(h, [&] {
         need(h->model_loaded && eta && chi, MGR_ERR_INVALID_ARG, "no model or NULL output");
@@ -1455,20 +1578,30 @@ mgr_status mgr_warm_start(mgr_handle *h, const mgr_mlp *net) {
              "network shape does not match the model (features, levels)");
         set_device(h);
         const int64_t N = h->N, np = mlp_param_count(net->nin, net->nout);
-        std::vector<void *> tmp;
-        struct Free {
-            std::vector<void *> &v;
-            ~Free() { for (void *p : v) cudaFree(p); }
-        } fr{tmp};
-        float *dF = dalloc<float>(h, N * MGR_MLP_FEATURES, &tmp);
-        float *dL = dalloc<float>(h, N * h->nlev, &tmp);
-        float *dD = dalloc<float>(h, N * h->nlev, &tmp);
+        if (!h->ws_F) {
+            h->ws_F = dalloc<float>(h, N * MGR_MLP_FEATURES, nullptr);
+            h->ws_L = dalloc<float>(h, N * h->nlev, nullptr);
+            h->ws_D = dalloc<float>(h, N * h->nlev, nullptr);
+            h->ws_mean = dalloc<float>(h, MGR_MLP_FEATURES, nullptr);
+            h->ws_istd = dalloc<float>(h, MGR_MLP_FEATURES, nullptr);
+        }
+        if (h->ws_np != np) {
+            free_ptr((void *&)h->ws_P);
+            h->ws_P = dalloc<float>(h, np, nullptr);
+            h->ws_np = np;
+        }
+        float *dF = h->ws_F, *dL = h->ws_L, *dD = h->ws_D, *P = h->ws_P;
         MlpDevice d;
         d.nin = net->nin;
         d.nout = net->nout;
-        float *P = upload(h, net->params, np, &tmp);
-        d.mean = upload(h, net->feat_mean, net->nin, &tmp);
-        d.istd = upload(h, net->feat_istd, net->nin, &tmp);
+        ck(cudaMemcpyAsync(P, net->params, np * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+           "network parameters");
+        ck(cudaMemcpyAsync(h->ws_mean, net->feat_mean, net->nin * sizeof(float),
+                           cudaMemcpyHostToDevice, h->stream), "feature mean");
+        ck(cudaMemcpyAsync(h->ws_istd, net->feat_istd, net->nin * sizeof(float),
+                           cudaMemcpyHostToDevice, h->stream), "feature scale");
+        d.mean = h->ws_mean;
+        d.istd = h->ws_istd;
         mlp_bind(P, d.nin, d.nout, d.W, d.b);
         ck(mlp_prepare(), "mlp attributes");
         device_features(h, dF);

@@ -54,10 +54,11 @@ __global__ void emissivity_opacity_kernel(ModelView m, LevelArgs a) {
     write_emissivity_opacity(m, a, p, k, a.pop + p * m.nlev);
 }
 
-// Simulation::compute_Jeff (Simulation/sim_lines.tpp:176-220), local ALO
+// Simulation::compute_Jeff (Simulation/sim_lines.tpp:176-220), local ALO,
+// for cells [c_begin, c_end)
 __global__ void jeff_kernel(ModelView m, LevelArgs a) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= m.N * m.nrad) return;
+    const int64_t idx = a.c_begin * m.nrad + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= a.c_end * m.nrad) return;
     const int64_t p = idx / m.nrad;
     const int k = (int)(idx - p * m.nrad);
     const double diff = a.Lam[idx] * a.pop[p * m.nlev + m.irad[k]];
@@ -113,9 +114,9 @@ __global__ void __launch_bounds__(kStateqWarps * 32) stateq_kernel(ModelView m, 
     __shared__ double popsh[kStateqWarps][kMaxLevels];
     __shared__ double red[kStateqWarps * 3];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t p = (int64_t)blockIdx.x * kStateqWarps + warp;
+    const int64_t p = a.c_begin + (int64_t)blockIdx.x * kStateqWarps + warp;
     // cells of a converged model of a batch keep their populations
-    const bool valid = p < m.N && !(m.seg_active && !m.seg_active[m.cell_seg[p]]);
+    const bool valid = p < a.c_end && !(m.seg_active && !m.seg_active[m.cell_seg[p]]);
     const int nl = m.nlev, K = m.nrad, last = nl - 1;
     double *M = Msh[warp];
     double *y = ysh[warp];
@@ -258,10 +259,25 @@ __global__ void __launch_bounds__(kStateqWarps * 32) stateq_kernel(ModelView m, 
     }
     block_reduce3(cnt, rsum, rmax, red);
     if (threadIdx.x == 0) {
-        a.partials[3 * blockIdx.x + 0] = cnt;
-        a.partials[3 * blockIdx.x + 1] = rsum;
-        a.partials[3 * blockIdx.x + 2] = rmax;
+        // at the global position of this block of cells
+        const int64_t g = a.c_begin / kStateqWarps + blockIdx.x;
+        a.partials[3 * g + 0] = cnt;
+        a.partials[3 * g + 1] = rsum;
+        a.partials[3 * g + 2] = rmax;
     }
+}
+
+// Population history of the cells outside [c_begin, c_end), shifted as the
+// statistical-equilibrium kernel shifts it for its own cells; their new
+// populations come from the shard that owns them.
+__global__ void history_shift_kernel(ModelView m, LevelArgs a) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m.N * m.nlev) return;
+    const int64_t p = q / m.nlev;
+    if (p >= a.c_begin && p < a.c_end) return;
+    a.prev3[q] = a.prev2[q];
+    a.prev2[q] = a.prev1[q];
+    a.prev1[q] = a.pop[q];
 }
 
 // Per-cell convergence partials (after an Ng step).
@@ -289,6 +305,8 @@ __global__ void convergence_partials_kernel(ModelView m, LevelArgs a) {
         a.partials[3 * blockIdx.x + 2] = rmax;
     }
 }
+
+static_assert(kStateqWarps == kCellsPerPartial, "one convergence partial per stateq block");
 
 // Final reduction of (count, sum, max) partials: stats[0] = fraction not
 // converged, stats[1] = mean relative change, stats[2] = max relative change.
@@ -414,16 +432,28 @@ cudaError_t launch_emissivity_opacity(const ModelView &m, const LevelArgs &a, cu
 }
 
 cudaError_t launch_jeff(const ModelView &m, const LevelArgs &a, cudaStream_t s) {
-    jeff_kernel<<<blocks_for(m.N * m.nrad, 256), 256, 0, s>>>(m, a);
+    if (a.c_end <= a.c_begin) return cudaSuccess;
+    jeff_kernel<<<blocks_for((a.c_end - a.c_begin) * m.nrad, 256), 256, 0, s>>>(m, a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_stateq(const ModelView &m, const LevelArgs &a, DevFlags *flags, cudaStream_t s) {
-    const unsigned blocks = blocks_for(m.N, kStateqWarps);
-    stateq_kernel<<<blocks, kStateqWarps * 32, 0, s>>>(m, a, flags);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    convergence_final_kernel<<<1, 1024, 0, s>>>(m, a, (int)blocks);
+    const bool whole = a.c_begin == 0 && a.c_end == m.N;
+    if (a.c_end > a.c_begin) {
+        stateq_kernel<<<blocks_for(a.c_end - a.c_begin, kStateqWarps), kStateqWarps * 32, 0, s>>>(
+            m, a, flags);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (!whole) {
+        history_shift_kernel<<<blocks_for(m.N * m.nlev, 256), 256, 0, s>>>(m, a);
+        return cudaGetLastError();
+    }
+    return launch_convergence_final(m, a, s);
+}
+
+cudaError_t launch_convergence_final(const ModelView &m, const LevelArgs &a, cudaStream_t s) {
+    convergence_final_kernel<<<1, 1024, 0, s>>>(m, a, (int)blocks_for(m.N, kStateqWarps));
     return cudaGetLastError();
 }
 

@@ -136,10 +136,12 @@ cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *c
                               double *shift, double *dZ, MixedPoint *mp, DevFlags *flags,
                               cudaStream_t s);
 // acc[0] = points of all traces, acc[1] = sum over (pair, origin) of ndep
-// where ndep > 1, acc[2] = the longest ray pair (points); pts_origin[N] and
+// where ndep > 1 for origins in [u_begin, u_end), acc[2] = the longest ray
+// pair (points); pts_origin[N] and
 // upd_origin[N] (updates of one formal solve per origin) when not null.
 cudaError_t launch_trace_stats(const ModelView &m, const int32_t *len, unsigned long long *acc,
-                               int32_t *pts_origin, float *upd_origin, cudaStream_t s);
+                               int32_t *pts_origin, float *upd_origin, int64_t u_begin,
+                               int64_t u_end, cudaStream_t s);
 
 struct SolveArgs {
     const double *eps, *kap;        // [N*K] emissivity, opacity (FP64 path)
@@ -151,6 +153,7 @@ struct SolveArgs {
     int4 *patch;                    // mixed: (origin, pair, bin) to redo in double
     unsigned long long *patch_count;
     int64_t patch_cap;
+    int64_t s_begin, s_end;         // origins of the trace store to solve: [s_begin, s_end)
 };
 // Formal solve of the origins of one trace store.  variant selects the
 // register budget (one of kSolveVariants compiled resident-block counts;
@@ -170,13 +173,21 @@ struct LevelArgs {
     double *partials;                      // reduction scratch
     double *stats;                         // [8] device results
     int npartials;
+    int64_t c_begin, c_end;                // cells whose Jeff and rate equations are solved
 };
 cudaError_t launch_lte(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_boundary_table(const ModelView &m, int64_t nboundary, const int64_t *b2c,
                                   double *table, cudaStream_t s);
 cudaError_t launch_emissivity_opacity(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_jeff(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+// Statistical equilibrium of cells [c_begin, c_end) (their convergence
+// partials at the global positions of their 4-cell blocks); the history of
+// the other cells is shifted as well.  With the whole cell range the
+// convergence statistics are reduced too; otherwise launch_convergence_final
+// reduces them once every shard's partials are in place.
 cudaError_t launch_stateq(const ModelView &m, const LevelArgs &a, DevFlags *flags, cudaStream_t s);
+cudaError_t launch_convergence_final(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+constexpr int kCellsPerPartial = 4;   // cells per convergence partial of launch_stateq
 cudaError_t launch_convergence(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_ng(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 int level_partials_needed(const ModelView &m);

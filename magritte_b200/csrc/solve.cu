@@ -497,8 +497,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     using Real = typename Pol::Real;
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
-    if (oi >= t.o_count) return;
+    const int64_t oi = a.s_begin + (int64_t)blockIdx.x * kWarpsPerBlock + warp;
+    if (oi >= a.s_end) return;
     const int o = (int)(t.o_begin + oi);
     if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
@@ -1004,8 +1004,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t oi = (int64_t)blockIdx.x * kWarpsPerBlock + warp;
-    if (oi >= t.o_count) return;
+    const int64_t oi = a.s_begin + (int64_t)blockIdx.x * kWarpsPerBlock + warp;
+    if (oi >= a.s_end) return;
     const int o = (int)(t.o_begin + oi);
     if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
@@ -1121,8 +1121,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
 cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const SolveArgs &a,
                                 int precision, int variant, DevFlags *flags, cudaStream_t s,
                                 int *kind) {
-    if (t.o_count == 0) return cudaSuccess;
-    const int64_t blocks = (t.o_count + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (a.s_end <= a.s_begin) return cudaSuccess;
+    const int64_t blocks = (a.s_end - a.s_begin + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const size_t shmem = (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
     // the staged kernels need each 32-bin chunk within two lines and lines
     // whose windows do not overlap

@@ -205,7 +205,8 @@ __global__ void __launch_bounds__(256) trace_stats_kernel(const int32_t *__restr
                                                           const int32_t *__restrict__ antipod,
                                                           int64_t N, int R, int npairs, int nfreqs,
                                                           unsigned long long *acc,
-                                                          int32_t *pts_origin, float *upd_origin) {
+                                                          int32_t *pts_origin, float *upd_origin,
+                                                          int64_t u_begin, int64_t u_end) {
     const int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long pts = 0, U = 0, mx = 0;
     if (o < N) {
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(256) trace_stats_kernel(const int32_t *__restr
         for (int r = 0; r < npairs; r++) {
             const unsigned long long ndep =
                 (unsigned)len[(int64_t)r * N + o] + (unsigned)len[(int64_t)antipod[r] * N + o] + 1ull;
-            if (ndep > 1) U += ndep;
+            if (ndep > 1 && o >= u_begin && o < u_end) U += ndep;
             mx = ndep - 1 > mx ? ndep - 1 : mx;
         }
         if (pts_origin) pts_origin[o] = (int32_t)pts;
@@ -236,12 +237,14 @@ __global__ void __launch_bounds__(256) trace_stats_kernel(const int32_t *__restr
 }  // namespace
 
 cudaError_t launch_trace_stats(const ModelView &m, const int32_t *len, unsigned long long *acc,
-                               int32_t *pts_origin, float *upd_origin, cudaStream_t s) {
+                               int32_t *pts_origin, float *upd_origin, int64_t u_begin,
+                               int64_t u_end, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(acc, 0, 3 * sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
     const int64_t blocks = (m.N + 255) / 256;
     trace_stats_kernel<<<(unsigned)blocks, 256, 0, s>>>(len, m.antipod, m.N, m.nrays, m.npairs,
-                                                        m.nfreqs, acc, pts_origin, upd_origin);
+                                                        m.nfreqs, acc, pts_origin, upd_origin,
+                                                        u_begin, u_end);
     return cudaGetLastError();
 }
 

@@ -38,6 +38,7 @@ class Simulation:
         if st != 0:
             raise MagritteError(st, "mgr_create failed (no CUDA device?)")
         self._h = h
+        self.device = device
         self.model = None
         self.error_max = []
         self.error_mean = []
@@ -131,6 +132,52 @@ class Simulation:
         self.error_max = list(hist[: it.value])
         self.converged = (st == 0)
         return int(it.value)
+
+    # ----------------------------------------------------- checkpoints
+    def population_history(self):
+        """(prev1, prev2, prev3): the iterates Ng acceleration reads."""
+        m = self.model
+        out = [np.zeros((m.ncells, m.linedata.nlev)) for _ in range(3)]
+        self._ck(self._lib.mgr_get_population_history(self._h, *[_capi.ptr(a) for a in out]))
+        return tuple(out)
+
+    def set_population_history(self, pop, prev1=None, prev2=None, prev3=None):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None
+                for a in (pop, prev1, prev2, prev3)]
+        self._ck(self._lib.mgr_set_population_history(
+            self._h, *[_capi.ptr(a) if a is not None else None for a in arrs]))
+
+    def write_checkpoint(self, folder: str, tag: str = ""):
+        """Populations and their history in Magritte's text layout
+        (``population<tag>``, ``population_prev1..3``, ``J_lin<tag>``,
+        ``J_eff<tag>`` of ``Lines/LineProducingSpecies_0/``)."""
+        from . import io_text
+        io_text.write_populations(folder, self.population, prev=self.population_history(),
+                                  Jlin=self.Jlin, Jeff=self.Jeff, tag=tag)
+
+    def read_checkpoint(self, folder: str, tag: str = ""):
+        """Restores what write_checkpoint (or the reference's
+        LineProducingSpecies::write) stored; the next
+        compute_level_populations continues where that run stopped."""
+        from . import io_text
+        d = io_text.read_populations(folder, tag)
+        self.set_population_history(d["population"], d.get("prev1"), d.get("prev2"),
+                                    d.get("prev3"))
+
+    # -------------------------------------------------- partitioned runs
+    def set_origin_range(self, begin: int, end: int):
+        """This handle solves origins (cells) [begin, end) only: one shard of
+        a run partitioned over GPUs (``magritte_b200.partition``)."""
+        self._ck(self._lib.mgr_set_origin_range(self._h, int(begin), int(end)))
+
+    def stateq_local(self):
+        """Jeff and statistical equilibrium of the shard's own cells."""
+        self._ck(self._lib.mgr_stateq_local(self._h))
+
+    def stateq_finish(self):
+        """Emissivities/opacities and convergence statistics after the
+        shards exchanged their populations and partials."""
+        self._ck(self._lib.mgr_stateq_finish(self._h))
 
     # ------------------------------------------------------ model batches
     def segment_results(self):

@@ -159,12 +159,14 @@ BATCH_MEMBERS = (30, 146, 122)   # three of the smallest members (about 2k point
 
 @pytest.fixture(scope="module")
 def batch_oracle():
-    """Each member alone through the oracle's ALI to 1e-6."""
+    """Each member alone through the oracle's ALI to 1e-5 (tighter targets
+    reach the region where the Ng coefficients are ill-conditioned and
+    last-bit differences change the trajectory, as for the cloud above)."""
     out = []
     for m in BATCH_MEMBERS:
         model = M.config4_member(m)
         orc = oracle.Oracle(model).setup()
-        it, _ = orc.compute_level_populations(True, 100, 1e-6, nthreads=THREADS)
+        it, _ = orc.compute_level_populations(True, 100, 1e-5, nthreads=THREADS)
         out.append((model, it, orc.pop.copy()))
     return out
 
@@ -174,7 +176,7 @@ def test_batch_members_vs_oracle(gpu, batch_oracle, precision, rtol):
     batch = M.concat_models([m for m, _, _ in batch_oracle], name="batch3")
     sim = device(batch)
     sim.compute_LTE_level_populations()
-    sim.compute_level_populations(True, 100, precision, tol_max_rel=1e-6, use_graph=True)
+    sim.compute_level_populations(True, 100, precision, tol_max_rel=1e-5, use_graph=True)
     assert sim.converged
     _, iters = sim.segment_results()
     pop = sim.population
