@@ -321,6 +321,25 @@ mgr_status mgr_mlp_loss_grad(int device, const mgr_mlp *net, const float *X, con
 
 /* --- without allocation ------------------------------------------------- */
 
+/* --- images -------------------------------------------------------------- */
+
+/* An image along ray `ray`: the emergent intensity through every cell, on
+ * the image grid nu[f] = line + line*width*root (the same in every cell,
+ * sorted ascending; width is relative, e.g. a few times v_max/c).  For each
+ * origin both rays are traced in the rest frame, the antipode's trace in
+ * front, and the ray pair is solved in FP64 with the current populations;
+ * I_m is the intensity leaving through the front (far end of the antipode's
+ * trace), I_p the one leaving through the end (far end of the ray's trace).
+ * ImX, ImY: each cell's coordinates on the image plane.  Replaces
+ * Simulation::compute_spectral_discretisation_image (sim_spectrum.tpp:200-250)
+ * + compute_boundary_intensities + compute_and_write_image
+ * (Simulation/sim_radiation.tpp:348-478, Image::set_coordinates in
+ * Simulation/Image/image.cpp:86-127).  Outputs: nu [nfreqs], I_m and I_p
+ * [ncells*nfreqs], ImX and ImY [ncells]; any may be NULL.  The radiation
+ * field's own grid and boundary table are left unchanged. */
+mgr_status mgr_compute_image(mgr_handle *h, int64_t ray, double width, double *nu, double *I_m,
+                             double *I_p, double *ImX, double *ImY);
+
 /* --- partitioned runs (one shard per GPU) -------------------------------- */
 
 /* Restricts the handle to the origins [o_begin, o_end) of its model: the

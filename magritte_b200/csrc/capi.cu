@@ -93,6 +93,7 @@ struct mgr_handle {
     int32_t *pts_origin_d = nullptr;   // [N] points of each origin's traces
     float *upd_origin_d = nullptr;     // [N] updates per origin (batches)
 
+    double pw_max = 0.0, vmax = 0.0;  // largest profile width (over c) and speed (over c)
     bool model_loaded = false, line_set = false, bdy_set = false, pops_valid = false;
     bool keep_J = false;
     double last_solve_ms = 0.0, last_updates = 0.0;
@@ -378,6 +379,9 @@ void do_upload(mgr_handle *h, const mgr_model_desc *d) {
         const double *v = d->velocity + 3 * p;
         vmax = std::max(vmax, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
     }
+
+    h->pw_max = pw_max;
+    h->vmax = vmax;
 
     // lines: the device path keeps the transitions' order, which must be
     // ascending in frequency (Lines::setup's heapsort then is the identity)
@@ -1612,6 +1616,119 @@ mgr_status mgr_warm_start(mgr_handle *h, const mgr_mlp *net) {
         h->launches += 4;
         ck(cudaStreamSynchronize(h->stream), "warm start sync");
         h->pops_valid = true;
+    });
+}
+
+mgr_status mgr_compute_image(mgr_handle *h, int64_t ray, double width, double *nu, double *I_m,
+                             double *I_p, double *ImX, double *ImY) {
+    return run(h, [&] {
+        need(h->model_loaded && h->pops_valid, MGR_ERR_STATE, "model and populations first");
+        need(ray >= 0 && ray < h->nrays, MGR_ERR_INVALID_ARG, "ray out of range");
+        need(width > 0.0 && std::isfinite(width), MGR_ERR_INVALID_ARG, "width must be positive");
+        set_device(h);
+        const int64_t N = h->N;
+        const int K = h->nrad, nq = h->nquads, nf = h->nfreqs;
+        // the image grid (Simulation::compute_spectral_discretisation_image,
+        // sim_spectrum.tpp:200-250): line + line*width*root, sorted
+        std::vector<double> line(K), roots(nq), grid(nf);
+        ck(cudaMemcpy(line.data(), h->mv.line, K * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(roots.data(), h->mv.roots, nq * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        for (int k = 0; k < K; k++)
+            for (int z = 0; z < nq; z++) {
+                volatile double lw = line[k] * width;
+                volatile double a = lw * roots[z];
+                grid[k * nq + z] = line[k] + a;
+            }
+        std::sort(grid.begin(), grid.end());
+        // lines each bin can reach: a traced point sees shift * nu with
+        // |shift - 1| <= vmax, the origin nu itself; +-11 widths
+        std::vector<int32_t> lo(nf), hi(nf);
+        const double sd = h->vmax * (1.0 + 1e-9) + 1e-15;
+        for (int f = 0; f < nf; f++) {
+            const double flo = grid[f] * (1.0 - sd) * (1.0 - 1e-12);
+            const double fhi = grid[f] * (1.0 + sd) * (1.0 + 1e-12);
+            int l0 = K, l1 = -1;
+            for (int l = 0; l < K; l++) {
+                const double wl = line[l] * (1.0 - 11.0 * h->pw_max) * (1.0 - 1e-12);
+                const double wh = line[l] * (1.0 + 11.0 * h->pw_max) * (1.0 + 1e-12);
+                if (fhi >= wl && flo <= wh) { l0 = std::min(l0, l); l1 = std::max(l1, l); }
+            }
+            lo[f] = l0 < K ? l0 : 0;
+            hi[f] = l1;
+        }
+        // the two rest-frame traces of every origin: the antipode in front
+        const int64_t ar = h->antipod[ray];
+        need(ar >= 0, MGR_ERR_INVALID_ARG, "the ray has no antipode");
+        auto ray_correct = [&](int64_t r) { return r >= h->nrays / 2 ? h->antipod[r] : r; };
+        std::vector<void *> tmp;
+        struct Free {
+            std::vector<void *> &v;
+            ~Free() { for (void *p : v) cudaFree(p); }
+        } fr{tmp};
+        int32_t *len = dalloc<int32_t>(h, 2 * N, &tmp);
+        int64_t *off = dalloc<int64_t>(h, 2 * N, &tmp);
+        reset_flags(h);
+        ck(launch_image_trace_count(h->mv, (int)ar, (int)ray, (int)ray_correct(ar),
+                                    (int)ray_correct(ray), len, h->flags, h->stream), "image trace");
+        h->launches += 1;
+        check_flags(h, "image trace");
+        const int64_t total = scan_lengths(h, len, off, 2 * N);
+        int32_t *cell = dalloc<int32_t>(h, total, &tmp);
+        double *shift = dalloc<double>(h, total, &tmp);
+        double *dZ = dalloc<double>(h, total, &tmp);
+        ck(launch_image_trace_fill(h->mv, (int)ar, (int)ray, (int)ray_correct(ar),
+                                   (int)ray_correct(ray), len, off, cell, shift, dZ, h->flags,
+                                   h->stream), "image trace fill");
+        h->launches += 1;
+        check_flags(h, "image trace fill");
+        ImageArgs a{};
+        double *dgrid = upload(h, grid.data(), nf, &tmp);
+        a.grid = dgrid;
+        a.lo = upload(h, lo.data(), nf, &tmp);
+        a.hi = upload(h, hi.data(), nf, &tmp);
+        double *table = dalloc<double>(h, h->nboundary * (int64_t)nf, &tmp);
+        ck(launch_image_table(h->mv, h->nboundary, h->b2c_dev, dgrid, nf, table, h->stream),
+           "image boundary");
+        a.table = table;
+        a.len = len;
+        a.off = off;
+        a.cell = cell;
+        a.shift = shift;
+        a.dZ = dZ;
+        a.eps = h->eps;
+        a.kap = h->kap;
+        a.I_m = dalloc<double>(h, N * nf, &tmp);
+        a.I_p = dalloc<double>(h, N * nf, &tmp);
+        a.nf = nf;
+        reset_flags(h);
+        ck(launch_image(h->mv, a, h->flags, h->stream), "image");
+        h->launches += 2;
+        check_flags(h, "image");
+        if (I_m) ck(cudaMemcpy(I_m, a.I_m, N * nf * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        if (I_p) ck(cudaMemcpy(I_p, a.I_p, N * nf * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        if (nu) std::copy(grid.begin(), grid.end(), nu);
+        // Image::set_coordinates (Simulation/Image/image.cpp:86-127)
+        if (ImX || ImY) {
+            std::vector<double> pos(3 * N), rr(3);
+            ck(cudaMemcpy(pos.data(), h->mv.pos, 3 * N * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+            ck(cudaMemcpy(rr.data(), h->mv.rays + 3 * ray, 3 * sizeof(double), cudaMemcpyDeviceToHost),
+               "d2h");
+            const double rx = rr[0], ry = rr[1], rz = rr[2];
+            const double den = std::sqrt(rx * rx + ry * ry);
+            for (int64_t p = 0; p < N; p++) {
+                const double x = pos[3 * p], y = pos[3 * p + 1], zz = pos[3 * p + 2];
+                double X = x, Y = y;
+                if (den != 0.0) {
+                    const double iden = 1.0 / den;
+                    const double ix = ry * iden, iy = -rx * iden;
+                    const double jx = rx * rz * iden, jy = ry * rz * iden, jz = -den;
+                    X = ix * x + iy * y;
+                    Y = jx * x + jy * y + jz * zz;
+                }
+                if (ImX) ImX[p] = X;
+                if (ImY) ImY[p] = Y;
+            }
+        }
     });
 }
 

@@ -128,6 +128,31 @@ struct DevFlags {
     unsigned long long patch_overflow;  // mixed entries beyond the patch list
 };
 
+// Emissivity and opacity at (cell p, frequency freq) over lines [lo, hi]:
+// Simulation::get_eta_and_chi (simulation.tpp:385-481) over the lines in the
+// bin's window, with Thermodynamics::profile (thermodynamics.tpp:16-29);
+// 1/exp(x^2) is written exp(-x^2) and 1/width (1/line)(1/pw).
+__device__ __forceinline__ void eta_chi_double(const ModelView &m, const double *__restrict__ eps,
+                                               const double *__restrict__ kap, int p, double freq,
+                                               int lo, int hi, double &eta, double &chi) {
+    eta = 0.0;
+    chi = 1.0E-26;
+    const double pwp = __ldg(m.pw + p);
+    const double ipw = __ldg(m.inv_pw + p);
+    const int K = m.nrad;
+    for (int l = lo; l <= hi; l++) {
+        const double line_l = __ldg(m.line + l);
+        const double width = line_l * pwp;
+        const double diff = freq - line_l;
+        const bool in = diff <= 11.0 * width && diff >= -11.0 * width;
+        const double inv_w = __ldg(m.inv_line + l) * ipw;
+        const double x = inv_w * diff;
+        const double fp = in ? freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x))) : 0.0;
+        eta += __ldg(eps + (unsigned)p * K + l) * fp;
+        chi += __ldg(kap + (unsigned)p * K + l) * fp;
+    }
+}
+
 // ------------------------------------------------------------------------
 // Host-side launchers (each file owns its kernels).
 cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_count,
@@ -135,6 +160,35 @@ cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_co
 cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
                               double *shift, double *dZ, MixedPoint *mp, DevFlags *flags,
                               cudaStream_t s);
+// Rest-frame traces of the two rays of an image for every origin: slot
+// d * N + o walks ray_front (d = 0) or ray_back (d = 1), its shift projected
+// on ray shift_front or shift_back.
+cudaError_t launch_image_trace_count(const ModelView &m, int ray_front, int ray_back,
+                                     int shift_front, int shift_back, int32_t *len,
+                                     DevFlags *flags, cudaStream_t s);
+cudaError_t launch_image_trace_fill(const ModelView &m, int ray_front, int ray_back,
+                                    int shift_front, int shift_back, const int32_t *len,
+                                    const int64_t *off, int32_t *cell, double *shift, double *dZ,
+                                    DevFlags *flags, cudaStream_t s);
+
+// Images (image.cu): the emergent intensities at both far ends of the ray
+// pair through every origin, on an image frequency grid common to all cells.
+struct ImageArgs {
+    const double *grid;        // [nf] image frequencies, ascending
+    const int32_t *lo, *hi;    // [nf] lines whose window can reach the bin
+    const double *table;       // [nboundary][nf] boundary intensities on the grid
+    const int32_t *len;        // [2N] trace lengths: front (antipode) then back
+    const int64_t *off;        // [2N]
+    const int32_t *cell;
+    const double *shift, *dZ;
+    const double *eps, *kap;   // [N*nrad]
+    double *I_m, *I_p;         // [N*nf]
+    int nf;
+};
+cudaError_t launch_image_table(const ModelView &m, int64_t nboundary, const int64_t *b2c,
+                               const double *grid, int nf, double *table, cudaStream_t s);
+cudaError_t launch_image(const ModelView &m, const ImageArgs &a, DevFlags *flags, cudaStream_t s);
+
 // acc[0] = points of all traces, acc[1] = sum over (pair, origin) of ndep
 // where ndep > 1 for origins in [u_begin, u_end), acc[2] = the longest ray
 // pair (points); pts_origin[N] and

@@ -144,31 +144,6 @@ __device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
 
 // ---------------------------------------------------------------- policies
 
-// Emissivity and opacity at (cell p, frequency freq) over lines [lo, hi]:
-// Simulation::get_eta_and_chi (simulation.tpp:385-481) over the lines in the
-// bin's window, with Thermodynamics::profile (thermodynamics.tpp:16-29);
-// 1/exp(x^2) is written exp(-x^2) and 1/width (1/line)(1/pw).
-__device__ __forceinline__ void eta_chi_double(const ModelView &m, const double *__restrict__ eps,
-                                               const double *__restrict__ kap, int p, double freq,
-                                               int lo, int hi, double &eta, double &chi) {
-    eta = 0.0;
-    chi = 1.0E-26;
-    const double pwp = __ldg(m.pw + p);
-    const double ipw = __ldg(m.inv_pw + p);
-    const int K = m.nrad;
-    for (int l = lo; l <= hi; l++) {
-        const double line_l = __ldg(m.line + l);
-        const double width = line_l * pwp;
-        const double diff = freq - line_l;
-        const bool in = diff <= 11.0 * width && diff >= -11.0 * width;
-        const double inv_w = __ldg(m.inv_line + l) * ipw;
-        const double x = inv_w * diff;
-        const double fp = in ? freq * (inv_w * kINVERSE_SQRT_PI * exp(-(x * x))) : 0.0;
-        eta += __ldg(eps + (unsigned)p * K + l) * fp;
-        chi += __ldg(kap + (unsigned)p * K + l) * fp;
-    }
-}
-
 template <bool kOverlap>
 struct Fp64Policy {
     using Real = double;

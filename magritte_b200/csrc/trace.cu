@@ -23,22 +23,33 @@ namespace {
 struct Walker {
     const ModelView &m;
     int64_t origin;
-    double rx, ry, rz;
+    double rx, ry, rz;       // direction of the walk
+    double sx, sy, sz;       // direction the Doppler shift is projected on
     double ox, oy, oz;       // origin position
-    double vox, voy, voz;    // origin velocity
+    double vox, voy, voz;    // origin velocity (zero in the rest frame)
 
-    __device__ Walker(const ModelView &mv, int64_t o, int d) : m(mv), origin(o) {
+    // shift_dir < 0: co-moving frame; otherwise the rest frame with the
+    // shift projected on ray shift_dir (Geometry::get_doppler_shift<Rest>
+    // fixes it "up the ray": the first-half ray of the pair)
+    __device__ Walker(const ModelView &mv, int64_t o, int d, int shift_dir = -1) : m(mv), origin(o) {
         rx = m.rays[3 * d + 0]; ry = m.rays[3 * d + 1]; rz = m.rays[3 * d + 2];
         ox = m.pos[3 * o + 0]; oy = m.pos[3 * o + 1]; oz = m.pos[3 * o + 2];
-        vox = m.vel[3 * o + 0]; voy = m.vel[3 * o + 1]; voz = m.vel[3 * o + 2];
+        if (shift_dir < 0) {
+            sx = rx; sy = ry; sz = rz;
+            vox = m.vel[3 * o + 0]; voy = m.vel[3 * o + 1]; voz = m.vel[3 * o + 2];
+        } else {
+            sx = m.rays[3 * shift_dir + 0]; sy = m.rays[3 * shift_dir + 1];
+            sz = m.rays[3 * shift_dir + 2];
+            vox = voy = voz = 0.0;   // v - 0 is v exactly
+        }
     }
 
-    // Geometry::get_doppler_shift<CoMoving> (geometry.tpp:443-446)
+    // Geometry::get_doppler_shift<CoMoving> and <Rest> (geometry.tpp:433-465)
     __device__ __forceinline__ double shift(int64_t c) const {
         const double dx = rsub(m.vel[3 * c + 0], vox);
         const double dy = rsub(m.vel[3 * c + 1], voy);
         const double dz = rsub(m.vel[3 * c + 2], voz);
-        return rsub(1.0, rdot3(dx, dy, dz, rx, ry, rz));
+        return rsub(1.0, rdot3(dx, dy, dz, sx, sy, sz));
     }
 
     // Geometry::get_next_general (geometry.tpp:328-421)
@@ -87,12 +98,14 @@ struct WriteSink {
             cell[base + n] = (int32_t)c;
             shift[base + n] = s;
             dZ[base + n] = z;
-            MixedPoint q;
-            q.cell = (int32_t)c;
-            q.delta = (float)(s - 1.0);
-            q.dzs = (float)(z * half_inv_scale);
-            q.ipw = (float)inv_pw[c];
-            mp[base + n] = q;
+            if (mp) {
+                MixedPoint q;
+                q.cell = (int32_t)c;
+                q.delta = (float)(s - 1.0);
+                q.dzs = (float)(z * half_inv_scale);
+                q.ipw = (float)inv_pw[c];
+                mp[base + n] = q;
+            }
         } else {
             over = true;
         }
@@ -130,8 +143,8 @@ __device__ __forceinline__ bool set_data(int64_t crt, int64_t nxt, double shift_
 // error code: 1 no neighbour ahead, 2 too many interpolation points,
 // 3 step limit.
 template <class Sink>
-__device__ int walk(const ModelView &m, int64_t o, int d, Sink &sink) {
-    const Walker w(m, o, d);
+__device__ int walk(const ModelView &m, int64_t o, int d, Sink &sink, int shift_dir = -1) {
+    const Walker w(m, o, d, shift_dir);
     const double dsm = m.dshift_max[o];
     double Z = 0.0, dZ = 0.0;
     int64_t nxt = w.next(o, Z, dZ);
@@ -196,6 +209,45 @@ __global__ void __launch_bounds__(128) trace_fill_kernel(ModelView m, TraceView 
     if (sink.over || (code == 0 && sink.n != sink.cap)) atomicAdd(&flags->cap_err, 1ull);
 }
 
+// Rest-frame traces of the two rays of one image (Simulation::
+// compute_and_write_image, sim_radiation.tpp:398-399): direction slot d of
+// origin o walks ray dirs[d]; idx = d * N + o.
+__global__ void __launch_bounds__(128) image_trace_count_kernel(ModelView m, int2 dirs,
+                                                                int2 sdirs, int32_t *len,
+                                                                DevFlags *flags) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 2 * m.N) return;
+    const int d = (int)(idx / m.N);
+    const int64_t o = idx % m.N;
+    CountSink sink;
+    const int code = walk(m, o, d == 0 ? dirs.x : dirs.y, sink, d == 0 ? sdirs.x : sdirs.y);
+    if (code) count_error(flags, code);
+    len[idx] = code ? 0 : (int32_t)sink.n;
+}
+
+__global__ void __launch_bounds__(128) image_trace_fill_kernel(ModelView m, int2 dirs,
+                                                               int2 sdirs, const int32_t *len,
+                                                               const int64_t *off, int32_t *cell,
+                                                               double *shift, double *dZ,
+                                                               DevFlags *flags) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 2 * m.N) return;
+    const int d = (int)(idx / m.N);
+    const int64_t o = idx % m.N;
+    WriteSink sink;
+    sink.cap = len[idx];
+    sink.base = off[idx];
+    sink.cell = cell;
+    sink.shift = shift;
+    sink.dZ = dZ;
+    sink.mp = nullptr;
+    sink.inv_pw = m.inv_pw;
+    sink.half_inv_scale = 0.0;
+    const int code = walk(m, o, d == 0 ? dirs.x : dirs.y, sink, d == 0 ? sdirs.x : sdirs.y);
+    if (code) count_error(flags, code);
+    if (sink.over || (code == 0 && sink.n != sink.cap)) atomicAdd(&flags->cap_err, 1ull);
+}
+
 // Statistics of a counted trace, one thread per origin: the points of every
 // direction, the ray-point sum of the formal solve's update count
 // (sum over pairs of ndep = n_r + n_ar + 1 where ndep > 1, as
@@ -245,6 +297,26 @@ cudaError_t launch_trace_stats(const ModelView &m, const int32_t *len, unsigned 
     trace_stats_kernel<<<(unsigned)blocks, 256, 0, s>>>(len, m.antipod, m.N, m.nrays, m.npairs,
                                                         m.nfreqs, acc, pts_origin, upd_origin,
                                                         u_begin, u_end);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_image_trace_count(const ModelView &m, int ray_front, int ray_back,
+                                     int shift_front, int shift_back, int32_t *len,
+                                     DevFlags *flags, cudaStream_t s) {
+    const int64_t blocks = (2 * m.N + 127) / 128;
+    image_trace_count_kernel<<<(unsigned)blocks, 128, 0, s>>>(
+        m, make_int2(ray_front, ray_back), make_int2(shift_front, shift_back), len, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_image_trace_fill(const ModelView &m, int ray_front, int ray_back,
+                                    int shift_front, int shift_back, const int32_t *len,
+                                    const int64_t *off, int32_t *cell, double *shift, double *dZ,
+                                    DevFlags *flags, cudaStream_t s) {
+    const int64_t blocks = (2 * m.N + 127) / 128;
+    image_trace_fill_kernel<<<(unsigned)blocks, 128, 0, s>>>(
+        m, make_int2(ray_front, ray_back), make_int2(shift_front, shift_back), len, off, cell,
+        shift, dZ, flags);
     return cudaGetLastError();
 }
 

@@ -133,6 +133,21 @@ class Simulation:
         self.converged = (st == 0)
         return int(it.value)
 
+    # ---------------------------------------------------------- images
+    def compute_image(self, ray: int, width: float) -> dict:
+        """Image along ``ray`` (``Simulation::compute_and_write_image``):
+        the image grid ``nu`` [nfreqs], emergent intensities ``I_m``/``I_p``
+        [ncells, nfreqs] through the front / end of each cell's ray pair,
+        and the image-plane coordinates ``ImX``/``ImY`` [ncells]."""
+        m = self.model
+        out = {"nu": np.zeros(m.nfreqs), "I_m": np.zeros((m.ncells, m.nfreqs)),
+               "I_p": np.zeros((m.ncells, m.nfreqs)), "ImX": np.zeros(m.ncells),
+               "ImY": np.zeros(m.ncells)}
+        self._ck(self._lib.mgr_compute_image(self._h, int(ray), float(width),
+                                             *[_capi.ptr(out[k]) for k in
+                                               ("nu", "I_m", "I_p", "ImX", "ImY")]))
+        return out
+
     # ----------------------------------------------------- checkpoints
     def population_history(self):
         """(prev1, prev2, prev3): the iterates Ng acceleration reads."""

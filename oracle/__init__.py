@@ -84,6 +84,10 @@ def lib():
         L.orc_compute_radiation_field.argtypes = [_P, _P, _P, _P, _i64, _i64, C.c_int]
         L.orc_solve_raypair.restype = None
         L.orc_solve_raypair.argtypes = [_i64, _i64, _P, _P, _dbl, _dbl, _P, _P]
+        L.orc_image_discretisation.restype = C.c_int
+        L.orc_image_discretisation.argtypes = [_P, _P, _dbl]
+        L.orc_compute_image.restype = C.c_int
+        L.orc_compute_image.argtypes = [_P, _P, _P, _i64, _P, _P, C.c_int]
         L.orc_compute_level_populations.restype = _i64
         L.orc_compute_level_populations.argtypes = [_P, _P, _P, C.c_int, _i64, _dbl, C.c_int, _P]
         _lib = L
@@ -229,6 +233,25 @@ class Oracle:
     def set_populations(self, pop: np.ndarray):
         self.pop[...] = pop
         lib().orc_set_emissivity_opacity(self.M, self.S)
+
+    # -------------------------------------------------------------- images
+    def compute_spectral_discretisation_image(self, width: float) -> int:
+        """The same grid line + line*width*root (sorted) in every cell
+        (sim_spectrum.tpp:200-250); the boundary table follows the grid."""
+        lib().orc_image_discretisation(self.M, self.S, float(width))
+        return lib().orc_boundary_intensities(self.M, self.S)
+
+    def compute_image(self, r: int, nthreads: int = 0):
+        """(I_m, I_p) [ncells, nfreqs] of compute_and_write_image for ray r
+        (sim_radiation.tpp:348-478)."""
+        m = self.m
+        I_m = np.zeros((m.ncells, m.nfreqs))
+        I_p = np.zeros((m.ncells, m.nfreqs))
+        err = lib().orc_compute_image(self.M, self.S, _ptr(self.antipod), int(r), _ptr(I_m),
+                                      _ptr(I_p), nthreads)
+        if err:
+            raise RuntimeError("trace error while imaging")
+        return I_m, I_p
 
     # ------------------------------------------------------------ geometry
     def dshift_max(self, o: int) -> float:

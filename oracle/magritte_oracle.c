@@ -176,12 +176,13 @@ static int set_data(int64_t crt, int64_t nxt, double shift_crt, double shift_nxt
     return 0;
 }
 
-/* Geometry::trace_ray<CoMoving>, Model/Geometry/geometry.tpp:21-95.
+/* Geometry::trace_ray<CoMoving> (rest = 0) or <Rest> (rest = 1),
+ * Model/Geometry/geometry.tpp:21-95.
  * err: 1 = no neighbour ahead before a boundary cell (the reference prints
  * "No proper neighbor found" and then reads out of bounds), 2 = more than
  * 10000 interpolation points on one step. */
-static void trace(const orc_model *m, int64_t origin, int64_t r, double dshift_max,
-                  trace_buf *t, int64_t *err)
+static void trace_frame(const orc_model *m, int64_t origin, int64_t r, double dshift_max,
+                        int rest, const int64_t *antipod, trace_buf *t, int64_t *err)
 {
     double Z = 0.0, dZ = 0.0;
     const double *ray = m->rays + 3 * r;
@@ -191,18 +192,24 @@ static void trace(const orc_model *m, int64_t origin, int64_t r, double dshift_m
     int64_t nxt = get_next_general(m, origin, ray, origin, &Z, &dZ);
     if (nxt != -1) {
         int64_t crt = origin;
-        double shift_crt = orc_doppler_shift(m, origin, r, crt, 0, NULL);
-        double shift_nxt = orc_doppler_shift(m, origin, r, nxt, 0, NULL);
+        double shift_crt = orc_doppler_shift(m, origin, r, crt, rest, antipod);
+        double shift_nxt = orc_doppler_shift(m, origin, r, nxt, rest, antipod);
         if (set_data(crt, nxt, shift_crt, shift_nxt, dZ, dshift_max, t)) { *err = 2; return; }
         while (!m->boundary[nxt]) {
             shift_crt = shift_nxt;
             crt = nxt;
             nxt = get_next_general(m, origin, ray, nxt, &Z, &dZ);
             if (nxt < 0) { *err = 1; return; }
-            shift_nxt = orc_doppler_shift(m, origin, r, nxt, 0, NULL);
+            shift_nxt = orc_doppler_shift(m, origin, r, nxt, rest, antipod);
             if (set_data(crt, nxt, shift_crt, shift_nxt, dZ, dshift_max, t)) { *err = 2; return; }
         }
     }
+}
+
+static void trace(const orc_model *m, int64_t origin, int64_t r, double dshift_max,
+                  trace_buf *t, int64_t *err)
+{
+    trace_frame(m, origin, r, dshift_max, 0, NULL, t, err);
 }
 
 int64_t orc_trace_ray(const orc_model *m, int64_t o, int64_t r, double dshift_max,
@@ -492,6 +499,69 @@ static inline double rescale_I_bdy(const orc_state *s, double freq_scaled, int64
     return (I2 - I1) / (nu2 - nu1) * (freq_scaled - nu1) + I1;
 }
 
+/* Simulation::setup (simulation.tpp:185-353) for bin f of origin o: the
+ * front trace's points (far end first), the origin, the back trace's
+ * points; term1 = eta/chi, dtau = (chi_n + chi_{n-1}) dZ / 2, the boundary
+ * intensities at both far ends (Radiation::rescale_I_bdy).  The origin is
+ * evaluated at its own grid frequency nu[o][f], every traced point at
+ * shift * nu[o][f].  Notches are carried per point across bins. */
+static void setup_pair(const orc_model *m, orc_state *s, const line_table *lt, int64_t o,
+                       int64_t f, const trace_buf *front, const trace_buf *back,
+                       raypair_buf *rb, int64_t *lnotch_at_origin, int64_t *first_out,
+                       int64_t *last_out, double *I0_out, double *In_out)
+{
+    const int64_t nf = s->nfreqs;
+    const int64_t n_ar = front->n, n_r = back->n;
+    double eta, chi, I_bdy_0, I_bdy_n;
+    int64_t first = 0, last = n_ar;
+    double freq_scaled = s->nu[o * nf + f];
+    int64_t index = n_ar;
+    get_eta_and_chi(m, s, lt, freq_scaled, o, lnotch_at_origin, &eta, &chi);
+    rb->term1[index] = eta / chi;
+    rb->chi[index] = chi; rb->nrs[index] = o; rb->frs[index] = freq_scaled;
+    double chi_prev = chi;
+    const double chi_o = chi;
+    if (n_ar > 0) {
+        index = n_ar - 1;
+        for (int64_t j = 0; j < n_ar; j++) {
+            freq_scaled = front->shift[j] * s->nu[o * nf + f];
+            get_eta_and_chi(m, s, lt, freq_scaled, front->cell[j], &rb->notch[j], &eta, &chi);
+            rb->term1[index] = eta / chi;
+            rb->dtau[index] = 0.5 * (chi + chi_prev) * front->dZ[j];
+            rb->chi[index] = chi; rb->nrs[index] = front->cell[j]; rb->frs[index] = freq_scaled;
+            chi_prev = chi;
+            index--;
+        }
+        const int64_t cellNr = front->cell[n_ar - 1];
+        I_bdy_0 = rescale_I_bdy(s, freq_scaled, cellNr, m->cell2boundary[cellNr]);
+        first = index + 1;
+        chi_prev = chi_o;
+    } else {
+        I_bdy_0 = s->I_bdy[m->cell2boundary[o] * nf + f];
+    }
+    if (n_r > 0) {
+        index = n_ar + 1;
+        for (int64_t j = 0; j < n_r; j++) {
+            freq_scaled = back->shift[j] * s->nu[o * nf + f];
+            get_eta_and_chi(m, s, lt, freq_scaled, back->cell[j], &rb->notch[n_ar + j], &eta, &chi);
+            rb->term1[index] = eta / chi;
+            rb->dtau[index - 1] = 0.5 * (chi + chi_prev) * back->dZ[j];
+            rb->chi[index] = chi; rb->nrs[index] = back->cell[j]; rb->frs[index] = freq_scaled;
+            chi_prev = chi;
+            index++;
+        }
+        const int64_t cellNr = back->cell[n_r - 1];
+        I_bdy_n = rescale_I_bdy(s, freq_scaled, cellNr, m->cell2boundary[cellNr]);
+        last = index - 1;
+    } else {
+        I_bdy_n = s->I_bdy[m->cell2boundary[o] * nf + f];
+    }
+    *first_out = first;
+    *last_out = last;
+    *I0_out = I_bdy_0;
+    *In_out = I_bdy_n;
+}
+
 /* One origin, one ray pair: Simulation::setup (simulation.tpp:185-353),
  * RayPair::solve, RayPair::update_Lambda (raypair_lambda.tpp:94-149) and the
  * J update (sim_radiation.tpp:150-264) for every frequency bin. */
@@ -516,50 +586,10 @@ static void solve_origin_pair(const orc_model *m, orc_state *s, const line_table
         int64_t lnotch_at_origin = 0;                      /* RayPair::initialize */
         for (int64_t i = 0; i < ndep; i++) rb->notch[i] = 0;  /* ProjectedCellData.lnotch */
         for (int64_t f = 0; f < nf; f++) {
-            double eta, chi, I_bdy_0, I_bdy_n;
-            int64_t first = 0, last = n_ar;
-            double freq_scaled = s->nu[o * nf + f];
-            int64_t index = n_ar;
-            get_eta_and_chi(m, s, lt, freq_scaled, o, &lnotch_at_origin, &eta, &chi);
-            rb->term1[index] = eta / chi;
-            rb->chi[index] = chi; rb->nrs[index] = o; rb->frs[index] = freq_scaled;
-            double chi_prev = chi;
-            const double chi_o = chi;
-            if (n_ar > 0) {
-                index = n_ar - 1;
-                for (int64_t j = 0; j < n_ar; j++) {
-                    freq_scaled = front->shift[j] * s->nu[o * nf + f];
-                    get_eta_and_chi(m, s, lt, freq_scaled, front->cell[j], &rb->notch[j], &eta, &chi);
-                    rb->term1[index] = eta / chi;
-                    rb->dtau[index] = 0.5 * (chi + chi_prev) * front->dZ[j];
-                    rb->chi[index] = chi; rb->nrs[index] = front->cell[j]; rb->frs[index] = freq_scaled;
-                    chi_prev = chi;
-                    index--;
-                }
-                const int64_t cellNr = front->cell[n_ar - 1];
-                I_bdy_0 = rescale_I_bdy(s, freq_scaled, cellNr, m->cell2boundary[cellNr]);
-                first = index + 1;
-                chi_prev = chi_o;
-            } else {
-                I_bdy_0 = s->I_bdy[m->cell2boundary[o] * nf + f];
-            }
-            if (n_r > 0) {
-                index = n_ar + 1;
-                for (int64_t j = 0; j < n_r; j++) {
-                    freq_scaled = back->shift[j] * s->nu[o * nf + f];
-                    get_eta_and_chi(m, s, lt, freq_scaled, back->cell[j], &rb->notch[n_ar + j], &eta, &chi);
-                    rb->term1[index] = eta / chi;
-                    rb->dtau[index - 1] = 0.5 * (chi + chi_prev) * back->dZ[j];
-                    rb->chi[index] = chi; rb->nrs[index] = back->cell[j]; rb->frs[index] = freq_scaled;
-                    chi_prev = chi;
-                    index++;
-                }
-                const int64_t cellNr = back->cell[n_r - 1];
-                I_bdy_n = rescale_I_bdy(s, freq_scaled, cellNr, m->cell2boundary[cellNr]);
-                last = index - 1;
-            } else {
-                I_bdy_n = s->I_bdy[m->cell2boundary[o] * nf + f];
-            }
+            double I_bdy_0, I_bdy_n;
+            int64_t first, last;
+            setup_pair(m, s, lt, o, f, front, back, rb, &lnotch_at_origin, &first, &last,
+                       &I_bdy_0, &I_bdy_n);
             double u, Ld;
             solve_raypair(rb, first, last, n_ar, I_bdy_0, I_bdy_n, &u, &Ld);
             if (s->appears[f]) {
@@ -628,6 +658,107 @@ int orc_compute_radiation_field(const orc_model *m, orc_state *s, const int64_t 
     }
     s->trace_errors = errs;
     free(lt.line); free(lt.line_index);
+    return errs ? 1 : 0;
+}
+
+/* ------------------------------------------------------------------ images */
+
+/* Simulation::compute_spectral_discretisation_image, Simulation/sim_spectrum.tpp:200-250:
+ * every cell gets the same grid, line + line*width*root over the sorted
+ * lines, sorted ascending. */
+int orc_image_discretisation(const orc_model *m, orc_state *s, double width)
+{
+    const int64_t nf = (int64_t)m->nrad * m->nquads;
+    double  *line = (double *)malloc(sizeof(double) * m->nrad);
+    int64_t *lidx = (int64_t *)malloc(sizeof(int64_t) * m->nrad);
+    double  *g    = (double *)malloc(sizeof(double) * nf);
+    sorted_lines(m, line, lidx);
+    s->nfreqs = nf;
+    int64_t index1 = 0;
+    for (int64_t k = 0; k < m->nrad; k++)
+        for (int64_t z = 0; z < m->nquads; z++) {
+            const double freqs_line = line[k];
+            g[index1++] = freqs_line + freqs_line * width * m->quad_roots[z];
+        }
+    for (int64_t i = 1; i < nf; i++) {
+        double v = g[i]; int64_t j = i - 1;
+        while (j >= 0 && g[j] > v) { g[j + 1] = g[j]; j--; }
+        g[j + 1] = v;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < m->ncells; p++)
+        memcpy(s->nu + p * nf, g, sizeof(double) * (size_t)nf);
+    free(line); free(lidx); free(g);
+    return 0;
+}
+
+/* Simulation::compute_and_write_image, Simulation/sim_radiation.tpp:348-478,
+ * for the ray r: per origin both rays traced in the rest frame
+ * (Geometry::trace_ray<Rest>), the antipode's trace in front, setup as for
+ * the radiation field, RayPair::solve_for_image
+ * (Simulation/Raypair/raypair_solver.tpp:523-579: elimination from the
+ * front, back substitution to the front) and the emergent intensities
+ * I_m = 2 u_front - I_bdy_0 and I_p = 2 u_end - I_bdy_n
+ * (RayPair::get_Im_at_front / get_Ip_at_end, raypair.tpp:205-229).  A ray
+ * pair of one point takes the boundary value of its bin.  I_m, I_p:
+ * [ncells*nfreqs]. */
+int orc_compute_image(const orc_model *m, orc_state *s, const int64_t *antipod, int64_t r,
+                      double *I_m, double *I_p, int nthreads)
+{
+    const int64_t nf = s->nfreqs;
+    const int64_t ar = antipod[r];
+    line_table lt;
+    lt.line = (double *)malloc(sizeof(double) * m->nrad);
+    lt.line_index = (int64_t *)malloc(sizeof(int64_t) * m->nrad);
+    sorted_lines(m, lt.line, lt.line_index);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    int64_t errs = 0;
+#pragma omp parallel reduction(+ : errs)
+    {
+        trace_buf tr = {0, 0, NULL, NULL, NULL, 1, 0};
+        trace_buf ta = {0, 0, NULL, NULL, NULL, 1, 0};
+        raypair_buf rb;
+        memset(&rb, 0, sizeof(rb));
+#pragma omp for schedule(static, 1)
+        for (int64_t o = 0; o < m->ncells; o++) {
+            const double dshift_max = orc_dshift_max(m, o);
+            int64_t e1 = 0, e2 = 0;
+            trace_frame(m, o, r, dshift_max, 1, antipod, &tr, &e1);
+            trace_frame(m, o, ar, dshift_max, 1, antipod, &ta, &e2);
+            if (e1 || e2) { errs++; continue; }
+            const int64_t ndep = ta.n + tr.n + 1;
+            if (ndep > 1) {
+                rp_ensure(&rb, ndep + 1);
+                int64_t lnotch_at_origin = 0;
+                for (int64_t i = 0; i < ndep; i++) rb.notch[i] = 0;
+                for (int64_t f = 0; f < nf; f++) {
+                    double I0, In, u, Ld;
+                    int64_t first, last;
+                    setup_pair(m, s, &lt, o, f, &ta, &tr, &rb, &lnotch_at_origin, &first, &last,
+                               &I0, &In);
+                    /* back substitution all the way to the front (n_ar = first) */
+                    solve_raypair(&rb, first, last, first, I0, In, &u, &Ld);
+                    I_m[o * nf + f] = 2.0 * rb.Su[0] - I0;
+                    I_p[o * nf + f] = 2.0 * rb.Su[ndep - 1] - In;
+                }
+            } else {
+                const int64_t b = m->cell2boundary[o];
+                for (int64_t f = 0; f < nf; f++) {
+                    I_m[o * nf + f] = s->I_bdy[b * nf + f];
+                    I_p[o * nf + f] = s->I_bdy[b * nf + f];
+                }
+            }
+        }
+        free(tr.cell); free(tr.shift); free(tr.dZ);
+        free(ta.cell); free(ta.shift); free(ta.dZ);
+        rp_free(&rb);
+    }
+    free(lt.line); free(lt.line_index);
+    s->trace_errors = errs;
     return errs ? 1 : 0;
 }
 

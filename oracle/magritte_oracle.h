@@ -122,6 +122,9 @@ void orc_lte(const orc_model *m, orc_state *s);
 void orc_set_emissivity_opacity(const orc_model *m, orc_state *s);
 
 /* formal solve over all ray pairs (or a subset of origins / pairs) */
+int orc_image_discretisation(const orc_model *m, orc_state *s, double width);
+int orc_compute_image(const orc_model *m, orc_state *s, const int64_t *antipod, int64_t r,
+                      double *I_m, double *I_p, int nthreads);
 int orc_compute_radiation_field(const orc_model *m, orc_state *s, const int64_t *antipod,
                                 const int64_t *origins, int64_t norigins,
                                 int64_t npairs, int nthreads);

@@ -14,12 +14,19 @@
 //                                              of every iteration
 //   magritte_ref <model/> <out/> trace <o...>  the traced points of every
 //                                              ray of the given origins
+//   magritte_ref <model/> <out/> image <r> <w> compute_and_write_image along
+//                                              ray r on the image grid of
+//                                              relative width w (LTE
+//                                              populations): written by the
+//                                              reference's Image::write
 //
 // The call sequence follows the reference's examples
 // (src/examples/example_1.cpp: read, compute_spectral_discretisation,
 // compute_boundary_intensities, compute_LTE_level_populations, ...), with
 // the boundary temperatures of the model folder passed to
 // compute_boundary_intensities (sim_radiation.tpp:17-40).
+#include <sys/stat.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -81,8 +88,9 @@ void write_populations(Simulation &sim, const std::string &out) {
 
 int main(int argc, char **argv) {
     if (argc < 4) {
-        std::fprintf(stderr, "usage: %s <model/> <out/> radiation [--pops] | ali <n> | trace <o>...\n",
-                     argv[0]);
+        std::fprintf(stderr,
+                     "usage: %s <model/> <out/> radiation [--pops] | ali <n> | trace <o>... | "
+                     "image <r> <width>\n", argv[0]);
         return 2;
     }
     const std::string model = argv[1], out = argv[2], cmd = argv[3];
@@ -134,6 +142,15 @@ int main(int argc, char **argv) {
         write_raw(out + "/trace_shift.bin", sh);
         write_raw(out + "/trace_dZ.bin", dz);
         return 0;
+    }
+    if (cmd == "image" && argc > 5) {
+        sim.compute_spectral_discretisation_image(std::atof(argv[5]));
+        sim.compute_boundary_intensities(sim.geometry.boundary.boundary_temperature);
+        sim.compute_LTE_level_populations();
+        mkdir((out + "/Simulation").c_str(), 0755);
+        mkdir((out + "/Simulation/Image").c_str(), 0755);
+        IoText io_out(out + "/");
+        return sim.compute_and_write_image(io_out, std::atol(argv[4]));
     }
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 2;

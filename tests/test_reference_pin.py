@@ -210,3 +210,19 @@ def test_population_checkpoint_round_trip(tmp_path):
     assert np.array_equal(back["population"], pop)
     for i in range(3):
         assert np.array_equal(back[f"prev{i + 1}"], prev[i])
+
+
+@needs_ref
+@pytest.mark.parametrize("make,ray,width", [(M.config1, 0, 2e-4), (small_wind, 1, 2e-5),
+                                            (small_turb, 3, 3e-5)])
+def test_image_matches_reference(tmp_path, make, ray, width):
+    """compute_and_write_image: rest-frame traces, solve_for_image, the
+    emergent intensities at both ends of every cell's ray pair."""
+    model = make()
+    out = run_ref(model, tmp_path, "image", str(ray), repr(width))
+    orc = oracle.Oracle(model).setup()
+    orc.compute_spectral_discretisation_image(width)
+    I_m, I_p = orc.compute_image(ray, nthreads=THREADS)
+    d = str(out) + "/"
+    assert rel(I_m, io_text.read_array(d, f"Simulation/Image/I_m_{ray}")) <= 1e-12
+    assert rel(I_p, io_text.read_array(d, f"Simulation/Image/I_p_{ray}")) <= 1e-12
