@@ -239,10 +239,17 @@ mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates);
 
 /* Mixed precision: (origin, pair, bin) solves of the last formal solve that
  * were redone in double (inverted lines driving the opacity below half its
- * 1e-26 floor, or a float failure), and the number of mixed solves since
- * mgr_create that were redone entirely in double because that list
- * overflowed.  No reference counterpart (the reference solves in double). */
+ * 1e-26 floor, or a float failure), and the number of origins since
+ * mgr_create that were solved again entirely in double because their
+ * failures did not fit that list.  No reference counterpart (the reference
+ * solves in double). */
 mgr_status mgr_get_patch_stats(mgr_handle *h, int64_t *patched, int64_t *fallbacks);
+
+/* Entries of the mixed solve's list of (origin, pair, bin) solves to redo
+ * in double (16 bytes each; 0 = automatic: 1 % of all solves, 1M to 64M
+ * entries).  Failures beyond it send their origins to a re-solve in
+ * double.  No reference counterpart. */
+mgr_status mgr_set_patch_capacity(mgr_handle *h, int64_t entries);
 
 /* Synchronises the handle's stream. */
 mgr_status mgr_synchronize(mgr_handle *h);
@@ -320,6 +327,35 @@ mgr_status mgr_mlp_loss_grad(int device, const mgr_mlp *net, const float *X, con
                              const float *target, int64_t n, float *loss, float *grad);
 
 /* --- without allocation ------------------------------------------------- */
+
+/* --- scattering ---------------------------------------------------------- */
+
+/* Scattering terms U and V of every ray pair, cell and bin
+ * ([nrays/2][ncells][nfreqs] host arrays; NULL sets zeros), as Radiation
+ * holds them (Model/Radiation/radiation.hpp:33-34). */
+mgr_status mgr_set_scattering_terms(mgr_handle *h, const double *U, const double *V);
+mgr_status mgr_get_scattering_terms(mgr_handle *h, double *U, double *V);
+
+/* The formal solve with scattering terms, FP64: every ray pair and origin
+ * set up as Simulation::setup_using_scattering (Simulation/simulation.tpp:51-171:
+ * term1 = (U + eta)/chi, term2 = V/chi, U and V interpolated on each cell's
+ * grid) and solved as RayPair::solve_using_scattering
+ * (Simulation/Raypair/raypair_solver.tpp:10-190) for u and v at the origin;
+ * J (when kept), Jlin and the ALO follow as in compute_radiation_field.
+ * The longer trace is in front, and v is stored with its sign flipped when
+ * that is the ray rather than its antipode (Simulation/sim_radiation.tpp:226-236).
+ * Needs the traces stored (within the trace budget).  The reference defines
+ * these two functions but its compute_radiation_field does not call them. */
+mgr_status mgr_compute_radiation_field_scattering(mgr_handle *h);
+
+/* u and v at the origins of the last scattering solve, [nrays/2][ncells][nfreqs]. */
+mgr_status mgr_get_scattering_uv(mgr_handle *h, double *u, double *v);
+
+/* U[r1] = sum over ray pairs r2 of u[r2] and V likewise, for every r1 (the
+ * phase function is one), from the last scattering solve: the scattering
+ * terms of the next one.  Replaces Radiation::calc_U_and_V
+ * (Model/Radiation/radiation.cpp:330-434, one process). */
+mgr_status mgr_calc_U_and_V(mgr_handle *h);
 
 /* --- images -------------------------------------------------------------- */
 

@@ -40,7 +40,9 @@ EXPORTS = (
     "mgr_set_segments", "mgr_get_segment_results", "mgr_set_autotune", "mgr_get_tuning",
     "mgr_get_patch_stats", "mgr_set_origin_range", "mgr_stateq_local", "mgr_stateq_finish",
     "mgr_get_device_buffer", "mgr_get_population_history", "mgr_set_population_history",
-    "mgr_compute_image",
+    "mgr_compute_image", "mgr_set_patch_capacity", "mgr_set_scattering_terms",
+    "mgr_get_scattering_terms", "mgr_compute_radiation_field_scattering", "mgr_get_scattering_uv",
+    "mgr_calc_U_and_V",
 )
 # mgr_buffer
 BUF_POPULATION, BUF_PREV1, BUF_PREV2, BUF_PREV3, BUF_JLIN, BUF_LAMBDA, BUF_PARTIALS = range(7)
@@ -149,6 +151,12 @@ def load(build_if_missing: bool = True):
     L.mgr_get_device_buffer.argtypes = [_P, _i32, C.POINTER(_P), C.POINTER(_i64)]
     L.mgr_get_population_history.argtypes = [_P, _P, _P, _P]
     L.mgr_compute_image.argtypes = [_P, _i64, _dbl, _P, _P, _P, _P, _P]
+    L.mgr_set_patch_capacity.argtypes = [_P, _i64]
+    L.mgr_set_scattering_terms.argtypes = [_P, _P, _P]
+    L.mgr_get_scattering_terms.argtypes = [_P, _P, _P]
+    L.mgr_compute_radiation_field_scattering.argtypes = [_P]
+    L.mgr_get_scattering_uv.argtypes = [_P, _P, _P]
+    L.mgr_calc_U_and_V.argtypes = [_P]
     L.mgr_set_population_history.argtypes = [_P, _P, _P, _P, _P]
     L.mgr_mlp_param_count.argtypes = [_i32, C.POINTER(_i64)]
     L.mgr_get_features.argtypes = [_P, _P]

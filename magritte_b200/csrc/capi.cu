@@ -106,8 +106,13 @@ struct mgr_handle {
     unsigned long long *patch_count = nullptr;
     unsigned long long *h_patch = nullptr;   // pinned copy of patch_count
     int64_t patch_cap = 0;
+    int64_t patch_cap_set = 0;         // capacity fixed by the caller (0: automatic)
     int64_t last_patched = 0;
-    int64_t fp64_fallbacks = 0;        // mixed solves redone in double (patch list full)
+    int64_t fp64_fallbacks = 0;        // origins re-solved in double (patch list full), cumulative
+    int32_t *redo_flag = nullptr, *redo_list = nullptr;   // [N] each
+
+    // scattering: terms U, V and the origins' u, v per (pair, cell, bin)
+    double *scat_U = nullptr, *scat_V = nullptr, *scat_u = nullptr, *scat_v = nullptr;
 
     // warm start: features, LTE log fractions, network output and the
     // network's parameters, kept between calls (allocated once per model)
@@ -225,14 +230,16 @@ void free_model(mgr_handle *h) {
     for (void *p : h->model_allocs) cudaFree(p);
     h->model_allocs.clear();
     void **ws[] = {(void **)&h->ws_F, (void **)&h->ws_L, (void **)&h->ws_D, (void **)&h->ws_P,
-                   (void **)&h->ws_mean, (void **)&h->ws_istd};
+                   (void **)&h->ws_mean, (void **)&h->ws_istd, (void **)&h->scat_U,
+                   (void **)&h->scat_V, (void **)&h->scat_u, (void **)&h->scat_v};
     for (void **p : ws) free_ptr(*p);
     h->ws_np = 0;
     void **state[] = {(void **)&h->pop, (void **)&h->prev1, (void **)&h->prev2, (void **)&h->prev3,
                       (void **)&h->eps, (void **)&h->kap, (void **)&h->Jlin, (void **)&h->Lam,
                       (void **)&h->Jeff, (void **)&h->J, (void **)&h->partials, (void **)&h->stats,
                       (void **)&h->ek, (void **)&h->flags, (void **)&h->ibdy,
-                      (void **)&h->patch, (void **)&h->patch_count};
+                      (void **)&h->patch, (void **)&h->patch_count, (void **)&h->redo_flag,
+                      (void **)&h->redo_list};
     for (void **p : state) free_ptr(*p);
     h->model_loaded = h->line_set = h->bdy_set = h->pops_valid = false;
 }
@@ -721,6 +728,9 @@ SolveArgs solve_args(mgr_handle *h) {
     a.patch_cap = h->patch_cap;
     a.s_begin = h->o_begin;   // origins of the stored trace (index = origin)
     a.s_end = h->o_end;
+    a.olist = nullptr;
+    a.redo_flag = h->redo_flag;
+    a.redo_list = h->redo_list;
     return a;
 }
 
@@ -733,11 +743,16 @@ void solve_prepare(mgr_handle *h, int precision) {
     if (!h->bdy_set) boundary_table(h);
     if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
     if (precision == MGR_MIXED && !h->patch) {
-        // room for 1 in 100 (origin, pair, bin) solves, 1M..64M entries
+        // room for 1 in 100 (origin, pair, bin) solves, 1M..64M entries,
+        // unless the caller fixed the capacity
         const double all = (double)h->N * h->npairs * h->nfreqs;
-        h->patch_cap = (int64_t)std::min(std::max(all / 100.0, (double)(1 << 20)), (double)(1 << 26));
+        h->patch_cap = h->patch_cap_set > 0 ? h->patch_cap_set
+                     : (int64_t)std::min(std::max(all / 100.0, (double)(1 << 20)), (double)(1 << 26));
         h->patch = dalloc<int4>(h, h->patch_cap, nullptr);
         h->patch_count = dalloc<unsigned long long>(h, 1, nullptr);
+        h->redo_flag = dalloc<int32_t>(h, h->N, nullptr);
+        h->redo_list = dalloc<int32_t>(h, h->N, nullptr);
+        ck(cudaMemset(h->redo_flag, 0, h->N * sizeof(int32_t)), "memset");
         h->gen++;
     }
 }
@@ -834,12 +849,31 @@ int graph_run(mgr_handle *h, mgr_handle::Graph &g, int key, const std::function<
     return g.kernels;
 }
 
+// Origins [done, count) of the redo list, whose float failures overflowed
+// the patch list, solved again entirely in double over the trace store t
+// (their Jlin, ALO and J are overwritten, after the patch pass added to
+// them).  Stream work only.
+void enqueue_redo(mgr_handle *h, const TraceView &t, int64_t done, int64_t count) {
+    if (count <= done) return;
+    SolveArgs a = solve_args(h);
+    a.olist = h->redo_list;
+    a.s_begin = done;
+    a.s_end = count;
+    int kind = 0;
+    ck(launch_formal_solve(h->mv, t, a, MGR_FP64, -1, h->flags, h->stream, &kind), "fp64 redo");
+    h->launches += 1;
+    h->fp64_fallbacks += count - done;
+}
+
 void finish_solve(mgr_handle *h, int precision, int variant, bool timing, int64_t patched) {
-    if (precision == MGR_MIXED && h->h_flags->patch_overflow) {
-        // more float failures than the patch list holds: solve in double
-        h->fp64_fallbacks++;
-        do_solve(h, MGR_FP64, false);
-        return;
+    if (precision == MGR_MIXED && h->stored && h->h_flags->redo_count > 0) {
+        // more float failures than the patch list holds: the listed origins
+        // again in double, then clear their marks for the next solve
+        TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
+        enqueue_redo(h, t, 0, (int64_t)h->h_flags->redo_count);
+        ck(cudaMemsetAsync(h->redo_flag, 0, h->N * sizeof(int32_t), h->stream), "redo reset");
+        ck(cudaEventRecord(h->ev1, h->stream), "event");
+        ck(cudaStreamSynchronize(h->stream), "fp64 redo");
     }
     check_flags(h, "formal solve");
     float ms = 0.f;
@@ -885,6 +919,7 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
     const SolveArgs a = solve_args(h);
     reset_flags(h);
     unsigned long long patched = 0;
+    int64_t redo_done = 0;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
     for (int64_t o0 = h->o_begin; o0 < h->o_end; o0 += h->batch_origins) {
         const int64_t cnt = std::min(h->batch_origins, h->o_end - o0);
@@ -902,10 +937,20 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
         if (precision == MGR_MIXED) {
             ck(cudaMemcpyAsync(h->h_patch, h->patch_count, sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, h->stream), "d2h");
+            ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost,
+                               h->stream), "flags");
             ck(cudaStreamSynchronize(h->stream), "patch count");
             patched += *h->h_patch;
+            // overflowing origins of this batch, in double, while its traces exist
+            const int64_t listed = (int64_t)h->h_flags->redo_count;
+            if (listed > redo_done) {
+                enqueue_redo(h, t, redo_done, listed);
+                redo_done = listed;
+            }
         }
     }
+    if (redo_done > 0)
+        ck(cudaMemsetAsync(h->redo_flag, 0, h->N * sizeof(int32_t), h->stream), "redo reset");
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream), "flags");
     ck(cudaStreamSynchronize(h->stream), "solve sync");
@@ -1504,6 +1549,20 @@ mgr_status mgr_get_patch_stats(mgr_handle *h, int64_t *patched, int64_t *fallbac
     });
 }
 
+mgr_status mgr_set_patch_capacity(mgr_handle *h, int64_t entries) {
+    return run(h, [&] {
+        need(entries >= 0, MGR_ERR_INVALID_ARG, "negative capacity");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        free_ptr((void *&)h->patch);
+        free_ptr((void *&)h->patch_count);
+        free_ptr((void *&)h->redo_flag);
+        free_ptr((void *&)h->redo_list);
+        h->patch_cap_set = entries;
+        h->gen++;
+    });
+}
+
 mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates) {
     return run(h, [&] {
         if (ms) *ms = h->last_solve_ms;
@@ -1729,6 +1788,99 @@ mgr_status mgr_compute_image(mgr_handle *h, int64_t ray, double width, double *n
                 if (ImY) ImY[p] = Y;
             }
         }
+    });
+}
+
+static int64_t scat_count(const mgr_handle *h) {
+    return (int64_t)h->npairs * h->N * h->nfreqs;
+}
+
+mgr_status mgr_set_scattering_terms(mgr_handle *h, const double *U, const double *V) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        set_device(h);
+        const int64_t n = scat_count(h);
+        if (!h->scat_U) {
+            h->scat_U = dalloc<double>(h, n, nullptr);
+            h->scat_V = dalloc<double>(h, n, nullptr);
+        }
+        if (U) ck(cudaMemcpy(h->scat_U, U, n * sizeof(double), cudaMemcpyHostToDevice), "h2d");
+        else ck(cudaMemset(h->scat_U, 0, n * sizeof(double)), "memset");
+        if (V) ck(cudaMemcpy(h->scat_V, V, n * sizeof(double), cudaMemcpyHostToDevice), "h2d");
+        else ck(cudaMemset(h->scat_V, 0, n * sizeof(double)), "memset");
+    });
+}
+
+mgr_status mgr_get_scattering_terms(mgr_handle *h, double *U, double *V) {
+    return run(h, [&] {
+        need(h->scat_U != nullptr, MGR_ERR_STATE, "no scattering terms yet");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        const int64_t n = scat_count(h);
+        if (U) ck(cudaMemcpy(U, h->scat_U, n * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        if (V) ck(cudaMemcpy(V, h->scat_V, n * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+    });
+}
+
+mgr_status mgr_compute_radiation_field_scattering(mgr_handle *h) {
+    return run(h, [&] {
+        need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
+        need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
+        need(h->scat_U != nullptr, MGR_ERR_STATE, "set the scattering terms first");
+        need(h->whole(), MGR_ERR_UNSUPPORTED, "the scattering solve runs on a whole model");
+        set_device(h);
+        if (!h->traced) do_trace(h);
+        need(h->stored, MGR_ERR_UNSUPPORTED,
+             "the scattering solve needs the traces stored (raise the trace budget)");
+        if (!h->bdy_set) boundary_table(h);
+        const int64_t n = scat_count(h);
+        if (!h->scat_u) {
+            h->scat_u = dalloc<double>(h, n, nullptr);
+            h->scat_v = dalloc<double>(h, n, nullptr);
+        }
+        if (h->keep_J && !h->J) h->J = dalloc<double>(h, h->N * (int64_t)h->nfreqs, nullptr);
+        ScatterArgs a{};
+        a.eps = h->eps;
+        a.kap = h->kap;
+        a.U = h->scat_U;
+        a.V = h->scat_V;
+        a.u = h->scat_u;
+        a.v = h->scat_v;
+        a.J = h->keep_J ? h->J : nullptr;
+        a.Jlin = h->Jlin;
+        a.Lam = h->Lam;
+        TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
+        reset_flags(h);
+        ck(cudaEventRecord(h->ev0, h->stream), "event");
+        ck(launch_scatter(h->mv, t, a, h->flags, h->stream), "scattering solve");
+        ck(cudaEventRecord(h->ev1, h->stream), "event");
+        h->launches += 1;
+        check_flags(h, "scattering solve");
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, h->ev0, h->ev1), "elapsed");
+        h->last_solve_ms = ms;
+        h->last_updates = h->updates_per_solve;
+    });
+}
+
+mgr_status mgr_get_scattering_uv(mgr_handle *h, double *u, double *v) {
+    return run(h, [&] {
+        need(h->scat_u != nullptr, MGR_ERR_STATE, "no scattering solve yet");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        const int64_t n = scat_count(h);
+        if (u) ck(cudaMemcpy(u, h->scat_u, n * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+        if (v) ck(cudaMemcpy(v, h->scat_v, n * sizeof(double), cudaMemcpyDeviceToHost), "d2h");
+    });
+}
+
+mgr_status mgr_calc_U_and_V(mgr_handle *h) {
+    return run(h, [&] {
+        need(h->scat_u != nullptr && h->scat_U != nullptr, MGR_ERR_STATE, "no scattering solve yet");
+        set_device(h);
+        ck(launch_calc_uv(h->mv, h->scat_u, h->scat_v, h->scat_U, h->scat_V, h->stream), "U and V");
+        h->launches += 1;
+        ck(cudaStreamSynchronize(h->stream), "sync");
     });
 }
 

@@ -126,6 +126,7 @@ struct DevFlags {
     unsigned long long cap_err;     // trace longer than its slot
     unsigned long long stuck_err;   // step limit reached
     unsigned long long patch_overflow;  // mixed entries beyond the patch list
+    unsigned long long redo_count;      // origins listed for an FP64 re-solve (overflow)
 };
 
 // Emissivity and opacity at (cell p, frequency freq) over lines [lo, hi]:
@@ -151,6 +152,69 @@ __device__ __forceinline__ void eta_chi_double(const ModelView &m, const double 
         eta += __ldg(eps + (unsigned)p * K + l) * fp;
         chi += __ldg(kap + (unsigned)p * K + l) * fp;
     }
+}
+
+// What the boundary condition needs, passed by value to the out-of-line
+// helper below.
+struct BdyCtx {
+    const int32_t *cell2bdy;
+    const double *ibdy;            // [nboundary][nfreqs] I_bdy on each boundary cell's grid
+    const double *pw, *line, *roots;
+    int nq, nf;
+};
+
+__device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
+    BdyCtx c;
+    c.cell2bdy = m.cell2bdy;
+    c.ibdy = m.ibdy;
+    c.pw = m.pw;
+    c.line = m.line;
+    c.roots = m.roots;
+    c.nq = m.nquads;
+    c.nf = m.nfreqs;
+    return c;
+}
+
+// Radiation::rescale_I_bdy (scalar build, Model/Radiation/radiation.tpp:341-373)
+// on the table of Simulation::compute_boundary_intensities.  The reference
+// takes the first bin of cell p's grid with freq <= nu_p(f) by a linear
+// search; the grid ascends (lines do not interleave, which the spectral
+// discretisation checks), so the same bin is found by bisection: first the
+// line whose last bin is >= freq, then the bin within that line.
+static __device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p,
+                                                         DevFlags *flags) {
+    const int b = __ldg(c.cell2bdy + p);
+    if (b < 0) {
+        atomicAdd(&flags->trace_err, 1ull);
+        return 0.0;
+    }
+    const double pwp = __ldg(c.pw + p);
+    const int nq = c.nq, nf = c.nf, K = nf / nq;
+    auto nu_kz = [&](int k, int z) {
+        const double line = __ldg(c.line + k);
+        return radd(line, rmul(rmul(line, pwp), __ldg(c.roots + z)));
+    };
+    int lo = 0, hi = K;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (freq <= nu_kz(mid, nq - 1)) hi = mid;
+        else lo = mid + 1;
+    }
+    const double *I = c.ibdy + (int64_t)b * nf;
+    if (lo == K) return __ldg(I + nf - 1);   // above the grid
+    const int k = lo;
+    int zl = 0, zh = nq - 1;
+    while (zl < zh) {
+        const int mid = (zl + zh) >> 1;
+        if (freq <= nu_kz(k, mid)) zh = mid;
+        else zl = mid + 1;
+    }
+    const int notch = k * nq + zl;
+    if (notch == 0 || notch == nf - 1) return __ldg(I + notch);
+    const double nu1 = nu_kz(k, zl);
+    const double nu2 = zl > 0 ? nu_kz(k, zl - 1) : nu_kz(k - 1, nq - 1);
+    const double I1 = __ldg(I + notch), I2 = __ldg(I + notch - 1);
+    return (I2 - I1) / (nu2 - nu1) * (freq - nu1) + I1;
 }
 
 // ------------------------------------------------------------------------
@@ -185,6 +249,20 @@ struct ImageArgs {
     double *I_m, *I_p;         // [N*nf]
     int nf;
 };
+// The formal solve with scattering terms (scatter.cu): U, V [npairs][N*nf]
+// in, u, v at the origins [npairs][N*nf] out, with J (optional), Jlin and
+// the ALO.
+struct ScatterArgs {
+    const double *eps, *kap;
+    const double *U, *V;
+    double *u, *v;
+    double *J, *Jlin, *Lam;
+};
+cudaError_t launch_scatter(const ModelView &m, const TraceView &t, const ScatterArgs &a,
+                           DevFlags *flags, cudaStream_t s);
+cudaError_t launch_calc_uv(const ModelView &m, const double *u, const double *v, double *U,
+                           double *V, cudaStream_t s);
+
 cudaError_t launch_image_table(const ModelView &m, int64_t nboundary, const int64_t *b2c,
                                const double *grid, int nf, double *table, cudaStream_t s);
 cudaError_t launch_image(const ModelView &m, const ImageArgs &a, DevFlags *flags, cudaStream_t s);
@@ -208,6 +286,9 @@ struct SolveArgs {
     unsigned long long *patch_count;
     int64_t patch_cap;
     int64_t s_begin, s_end;         // origins of the trace store to solve: [s_begin, s_end)
+    const int32_t *olist;           // when set: solve origins olist[s_begin .. s_end) instead
+    int32_t *redo_flag;             // [N] mixed: 1 once an origin is listed for an FP64 re-solve
+    int32_t *redo_list;             // [N] mixed: origins whose failures overflowed the patch list
 };
 // Formal solve of the origins of one trace store.  variant selects the
 // register budget (one of kSolveVariants compiled resident-block counts;

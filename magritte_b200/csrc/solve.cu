@@ -80,68 +80,6 @@ struct BinCtx {
     float q;          // pw_o * root_z: offset of the bin from its line, in units of nu
 };
 
-// What the boundary condition needs, passed by value to the out-of-line
-// helper below.
-struct BdyCtx {
-    const int32_t *cell2bdy;
-    const double *ibdy;            // [nboundary][nfreqs] I_bdy on each boundary cell's grid
-    const double *pw, *line, *roots;
-    int nq, nf;
-};
-
-// Radiation::rescale_I_bdy (scalar build, Model/Radiation/radiation.tpp:341-373)
-// on the table of Simulation::compute_boundary_intensities.  The reference
-// takes the first bin of cell p's grid with freq <= nu_p(f) by a linear
-// search; the grid ascends (lines do not interleave, which the spectral
-// discretisation checks), so the same bin is found by bisection: first the
-// line whose last bin is >= freq, then the bin within that line.
-__device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p, DevFlags *flags) {
-    const int b = __ldg(c.cell2bdy + p);
-    if (b < 0) {
-        atomicAdd(&flags->trace_err, 1ull);
-        return 0.0;
-    }
-    const double pwp = __ldg(c.pw + p);
-    const int nq = c.nq, nf = c.nf, K = nf / nq;
-    auto nu_kz = [&](int k, int z) {
-        const double line = __ldg(c.line + k);
-        return radd(line, rmul(rmul(line, pwp), __ldg(c.roots + z)));
-    };
-    int lo = 0, hi = K;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (freq <= nu_kz(mid, nq - 1)) hi = mid;
-        else lo = mid + 1;
-    }
-    const double *I = c.ibdy + (int64_t)b * nf;
-    if (lo == K) return __ldg(I + nf - 1);   // above the grid
-    const int k = lo;
-    int zl = 0, zh = nq - 1;
-    while (zl < zh) {
-        const int mid = (zl + zh) >> 1;
-        if (freq <= nu_kz(k, mid)) zh = mid;
-        else zl = mid + 1;
-    }
-    const int notch = k * nq + zl;
-    if (notch == 0 || notch == nf - 1) return __ldg(I + notch);
-    const double nu1 = nu_kz(k, zl);
-    const double nu2 = zl > 0 ? nu_kz(k, zl - 1) : nu_kz(k - 1, nq - 1);
-    const double I1 = __ldg(I + notch), I2 = __ldg(I + notch - 1);
-    return (I2 - I1) / (nu2 - nu1) * (freq - nu1) + I1;
-}
-
-__device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
-    BdyCtx c;
-    c.cell2bdy = m.cell2bdy;
-    c.ibdy = m.ibdy;
-    c.pw = m.pw;
-    c.line = m.line;
-    c.roots = m.roots;
-    c.nq = m.nquads;
-    c.nf = m.nfreqs;
-    return c;
-}
-
 // ---------------------------------------------------------------- policies
 
 template <bool kOverlap>
@@ -459,6 +397,16 @@ __device__ __noinline__ void patch_entry(const ModelView &m, const TraceView &t,
     if (a.J) atomicAdd(a.J + (int64_t)o * nf + f, 2.0 * wr * u);
 }
 
+// More float failures than the patch list holds: the origin is listed
+// (once) to be solved again entirely in double after the patch pass.
+__device__ __forceinline__ void list_for_redo(const SolveArgs &a, DevFlags *flags, int o) {
+    atomicAdd(&flags->patch_overflow, 1ull);
+    if (atomicExch(a.redo_flag + o, 1) == 0) {
+        const unsigned long long i = atomicAdd(&flags->redo_count, 1ull);
+        a.redo_list[i] = o;
+    }
+}
+
 __global__ void patch_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
     const int64_t n = min((unsigned long long)*a.patch_count, (unsigned long long)a.patch_cap);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -472,8 +420,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     using Real = typename Pol::Real;
     extern __shared__ double smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t oi = a.s_begin + (int64_t)blockIdx.x * kWarpsPerBlock + warp;
-    if (oi >= a.s_end) return;
+    const int64_t idx = a.s_begin + (int64_t)blockIdx.x * kWarpsPerBlock + warp;
+    if (idx >= a.s_end) return;
+    const int64_t oi = a.olist ? (int64_t)a.olist[idx] - t.o_begin : idx;
     const int o = (int)(t.o_begin + oi);
     if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
@@ -538,7 +487,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
                 // leave this pair to the double-precision patch pass
                 const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
                 if (slot < (unsigned long long)a.patch_cap) a.patch[slot] = make_int4(o, r, fc, 0);
-                else atomicAdd(&flags->patch_overflow, 1ull);
+                else list_for_redo(a, flags, o);
                 continue;
             }
             Jf += 2.0 * wr * u;
@@ -979,8 +928,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     formal_solve_staged_kernel(ModelView m, TraceView t, SolveArgs a, DevFlags *flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t oi = a.s_begin + (int64_t)blockIdx.x * kWarpsPerBlock + warp;
-    if (oi >= a.s_end) return;
+    const int64_t idx = a.s_begin + (int64_t)blockIdx.x * kWarpsPerBlock + warp;
+    if (idx >= a.s_end) return;
+    const int64_t oi = a.olist ? (int64_t)a.olist[idx] - t.o_begin : idx;
     const int o = (int)(t.o_begin + oi);
     if (m.seg_active && !m.seg_active[m.cell_seg[o]]) return;   // converged model of a batch
     const int K = m.nrad, nq = m.nquads, nf = m.nfreqs;
@@ -1063,7 +1013,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
             if (!kFp64 && !(isfinite(u) && isfinite(L))) {
                 const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
                 if (slot < (unsigned long long)a.patch_cap) a.patch[slot] = make_int4(o, r, fc, 0);
-                else atomicAdd(&flags->patch_overflow, 1ull);
+                else list_for_redo(a, flags, o);
                 continue;
             }
             Jf += 2.0 * wr * u;

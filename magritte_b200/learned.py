@@ -193,6 +193,9 @@ def main(argv=None):
     ap.add_argument("--seed0", type=int, default=100)
     ap.add_argument("--nlev", type=int, default=10)
     ap.add_argument("--epochs", type=int, default=600)
+    ap.add_argument("--max-iter", type=int, default=400,
+                    help="ALI cap of each training model; models that do not converge by it "
+                         "are left out of the training set")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "weights",
                                                   "wind_rotor10.npz"))
     a = ap.parse_args(argv)
@@ -202,7 +205,11 @@ def main(argv=None):
     rng = np.random.default_rng(a.seed0)
     for m in fam(a.n, a.models, a.seed0, a.nlev):
         t_m = time.time()
-        X, L, T, it = converged_samples(m)
+        X, L, T, it = converged_samples(m, max_iter=a.max_iter)
+        if it >= a.max_iter:
+            print(f"{m.name}: not converged in {it} iterations, left out", flush=True)
+            its.append(it)
+            continue
         if a.subsample < 1.0:
             keep = rng.random(X.shape[0]) < a.subsample
             X, L, T = X[keep], L[keep], T[keep]
@@ -214,7 +221,8 @@ def main(argv=None):
     hist = net.train(X, L, T, epochs=a.epochs)
     t2 = time.time()
     net.meta = dict(family=a.family, n=a.n, subsample=a.subsample, models=a.models, seed0=a.seed0, nlev=a.nlev,
-                    epochs=a.epochs, samples=int(X.shape[0]), final_loss=float(hist[-1]),
+                    epochs=a.epochs, max_iter=a.max_iter, samples=int(X.shape[0]),
+                    final_loss=float(hist[-1]),
                     first_loss=float(hist[0]), ali_iterations=its,
                     data_s=round(t1 - t0, 1), train_s=round(t2 - t1, 1))
     net.save(a.out)

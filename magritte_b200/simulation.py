@@ -133,6 +133,40 @@ class Simulation:
         self.converged = (st == 0)
         return int(it.value)
 
+    # ------------------------------------------------------ scattering
+    def _scat_shape(self):
+        m = self.model
+        return (m.nrays // 2, m.ncells, m.nfreqs)
+
+    def set_scattering_terms(self, U=None, V=None):
+        """Scattering terms U, V [nrays/2, ncells, nfreqs] (None: zeros)."""
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64).reshape(self._scat_shape())
+                for a in (U, V)]
+        self._ck(self._lib.mgr_set_scattering_terms(
+            self._h, *[None if a is None else _capi.ptr(a) for a in arrs]))
+
+    def scattering_terms(self):
+        U, V = np.zeros(self._scat_shape()), np.zeros(self._scat_shape())
+        self._ck(self._lib.mgr_get_scattering_terms(self._h, _capi.ptr(U), _capi.ptr(V)))
+        return U, V
+
+    def compute_radiation_field_scattering(self, keep_J: Optional[bool] = None) -> int:
+        """The formal solve with scattering terms
+        (``setup_using_scattering`` + ``solve_using_scattering``)."""
+        if keep_J is not None:
+            self._ck(self._lib.mgr_set_keep_J(self._h, int(bool(keep_J))))
+        return self._ck(self._lib.mgr_compute_radiation_field_scattering(self._h))
+
+    def scattering_uv(self):
+        """u and v at the origins of the last scattering solve."""
+        u, v = np.zeros(self._scat_shape()), np.zeros(self._scat_shape())
+        self._ck(self._lib.mgr_get_scattering_uv(self._h, _capi.ptr(u), _capi.ptr(v)))
+        return u, v
+
+    def calc_U_and_V(self):
+        """Next scattering terms from the last solve (``Radiation::calc_U_and_V``)."""
+        self._ck(self._lib.mgr_calc_U_and_V(self._h))
+
     # ---------------------------------------------------------- images
     def compute_image(self, ray: int, width: float) -> dict:
         """Image along ``ray`` (``Simulation::compute_and_write_image``):
@@ -210,6 +244,12 @@ class Simulation:
         a, b = C.c_int64(0), C.c_int64(0)
         self._ck(self._lib.mgr_get_patch_stats(self._h, C.byref(a), C.byref(b)))
         return int(a.value), int(b.value)
+
+    def set_patch_capacity(self, entries: int):
+        """Capacity of the mixed solve's list of solves redone in double
+        (0: automatic); origins whose failures overflow it are re-solved in
+        double."""
+        self._ck(self._lib.mgr_set_patch_capacity(self._h, int(entries)))
 
     # ------------------------------------------------------------ tuning
     def set_autotune(self, mode=True):

@@ -84,6 +84,10 @@ def lib():
         L.orc_compute_radiation_field.argtypes = [_P, _P, _P, _P, _i64, _i64, C.c_int]
         L.orc_solve_raypair.restype = None
         L.orc_solve_raypair.argtypes = [_i64, _i64, _P, _P, _dbl, _dbl, _P, _P]
+        L.orc_compute_radiation_field_scattering.restype = C.c_int
+        L.orc_compute_radiation_field_scattering.argtypes = [_P, _P, _P, _P, _P, _P, _P, C.c_int]
+        L.orc_calc_U_and_V.restype = None
+        L.orc_calc_U_and_V.argtypes = [_P, _P, _P, _P, _P, _P]
         L.orc_image_discretisation.restype = C.c_int
         L.orc_image_discretisation.argtypes = [_P, _P, _dbl]
         L.orc_compute_image.restype = C.c_int
@@ -233,6 +237,35 @@ class Oracle:
     def set_populations(self, pop: np.ndarray):
         self.pop[...] = pop
         lib().orc_set_emissivity_opacity(self.M, self.S)
+
+    # ---------------------------------------------------------- scattering
+    def compute_radiation_field_scattering(self, U, V, nthreads: int = 0):
+        """Every ray pair and origin through setup_using_scattering and
+        solve_using_scattering with scattering terms U, V
+        [nrays/2, ncells, nfreqs]; returns u, v at the origins (same shape).
+        J and the ALO are accumulated as in compute_radiation_field."""
+        m = self.m
+        shape = (m.nrays // 2, m.ncells, m.nfreqs)
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(shape)
+        V = np.ascontiguousarray(V, dtype=np.float64).reshape(shape)
+        u = np.zeros(shape)
+        v = np.zeros(shape)
+        err = lib().orc_compute_radiation_field_scattering(self.M, self.S, _ptr(self.antipod),
+                                                           _ptr(U), _ptr(V), _ptr(u), _ptr(v),
+                                                           nthreads)
+        if err:
+            raise RuntimeError("trace error")
+        return u, v
+
+    def calc_U_and_V(self, u, v):
+        m = self.m
+        shape = (m.nrays // 2, m.ncells, m.nfreqs)
+        u = np.ascontiguousarray(u, dtype=np.float64).reshape(shape)
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(shape)
+        U = np.zeros(shape)
+        V = np.zeros(shape)
+        lib().orc_calc_U_and_V(self.M, self.S, _ptr(u), _ptr(v), _ptr(U), _ptr(V))
+        return U, V
 
     # -------------------------------------------------------------- images
     def compute_spectral_discretisation_image(self, width: float) -> int:

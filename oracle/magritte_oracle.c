@@ -661,6 +661,268 @@ int orc_compute_radiation_field(const orc_model *m, orc_state *s, const int64_t 
     return errs ? 1 : 0;
 }
 
+/* --------------------------------------------------------------- scattering */
+
+/* Radiation::rescale_U_and_V (scalar build, Model/Radiation/radiation.tpp:232-262):
+ * U and V of ray pair R on cell p's grid, interpolated linearly at freq. */
+static inline void rescale_U_and_V(const orc_state *s, const double *U, const double *V,
+                                   int64_t ncells, double freq_scaled, int64_t R, int64_t p,
+                                   double *Us, double *Vs)
+{
+    const int64_t nf = s->nfreqs;
+    const double *Ur = U + R * ncells * nf + p * nf;
+    const double *Vr = V + R * ncells * nf + p * nf;
+    int64_t notch = 0;
+    search_with_notch(s->nu + p * nf, nf, &notch, freq_scaled);
+    if (notch == 0 || notch == nf - 1) { *Us = Ur[notch]; *Vs = Vr[notch]; return; }
+    const double nu1 = s->nu[p * nf + notch], nu2 = s->nu[p * nf + notch - 1];
+    *Us = (Ur[notch - 1] - Ur[notch]) / (nu2 - nu1) * (freq_scaled - nu1) + Ur[notch];
+    *Vs = (Vr[notch - 1] - Vr[notch]) / (nu2 - nu1) * (freq_scaled - nu1) + Vr[notch];
+}
+
+/* Simulation::setup_using_scattering (Simulation/simulation.tpp:51-171) for
+ * bin f: as setup, with RayPair::set_term1_and_term2 (raypair.tpp:86-100)
+ * term1 = (U + eta)/chi and term2 = V/chi (into term2[]); U and V at the
+ * origin are its own bin's, elsewhere interpolated (rescale_U_and_V). */
+static void setup_scattering(const orc_model *m, orc_state *s, const line_table *lt, int64_t o,
+                             int64_t f, int64_t R, const double *U, const double *V,
+                             const trace_buf *front, const trace_buf *back, raypair_buf *rb,
+                             double *term2, int64_t *lnotch_at_origin, double *I0_out,
+                             double *In_out)
+{
+    const int64_t nf = s->nfreqs, N = m->ncells;
+    const int64_t n_ar = front->n, n_r = back->n;
+    double eta, chi, Us, Vs;
+    double freq_scaled = s->nu[o * nf + f];
+    int64_t index = n_ar;
+    Us = U[R * N * nf + o * nf + f];
+    Vs = V[R * N * nf + o * nf + f];
+    get_eta_and_chi(m, s, lt, freq_scaled, o, lnotch_at_origin, &eta, &chi);
+    double inverse_chi = 1.0 / chi;
+    rb->term1[index] = (Us + eta) * inverse_chi;
+    term2[index] = Vs * inverse_chi;
+    rb->chi[index] = chi; rb->nrs[index] = o; rb->frs[index] = freq_scaled;
+    double chi_prev = chi;
+    const double chi_o = chi;
+    if (n_ar > 0) {
+        index = n_ar - 1;
+        for (int64_t j = 0; j < n_ar; j++) {
+            freq_scaled = front->shift[j] * s->nu[o * nf + f];
+            rescale_U_and_V(s, U, V, N, freq_scaled, R, front->cell[j], &Us, &Vs);
+            get_eta_and_chi(m, s, lt, freq_scaled, front->cell[j], &rb->notch[j], &eta, &chi);
+            inverse_chi = 1.0 / chi;
+            rb->term1[index] = (Us + eta) * inverse_chi;
+            term2[index] = Vs * inverse_chi;
+            rb->dtau[index] = 0.5 * (chi + chi_prev) * front->dZ[j];
+            rb->chi[index] = chi; rb->nrs[index] = front->cell[j]; rb->frs[index] = freq_scaled;
+            chi_prev = chi;
+            index--;
+        }
+        const int64_t cellNr = front->cell[n_ar - 1];
+        *I0_out = rescale_I_bdy(s, freq_scaled, cellNr, m->cell2boundary[cellNr]);
+        chi_prev = chi_o;
+    } else {
+        *I0_out = s->I_bdy[m->cell2boundary[o] * nf + f];
+    }
+    if (n_r > 0) {
+        index = n_ar + 1;
+        for (int64_t j = 0; j < n_r; j++) {
+            freq_scaled = back->shift[j] * s->nu[o * nf + f];
+            rescale_U_and_V(s, U, V, N, freq_scaled, R, back->cell[j], &Us, &Vs);
+            get_eta_and_chi(m, s, lt, freq_scaled, back->cell[j], &rb->notch[n_ar + j], &eta, &chi);
+            inverse_chi = 1.0 / chi;
+            rb->term1[index] = (Us + eta) * inverse_chi;
+            term2[index] = Vs * inverse_chi;
+            rb->dtau[index - 1] = 0.5 * (chi + chi_prev) * back->dZ[j];
+            rb->chi[index] = chi; rb->nrs[index] = back->cell[j]; rb->frs[index] = freq_scaled;
+            chi_prev = chi;
+            index++;
+        }
+        const int64_t cellNr = back->cell[n_r - 1];
+        *In_out = rescale_I_bdy(s, freq_scaled, cellNr, m->cell2boundary[cellNr]);
+    } else {
+        *In_out = s->I_bdy[m->cell2boundary[o] * nf + f];
+    }
+}
+
+/* RayPair::solve_using_scattering (Simulation/Raypair/raypair_solver.tpp:10-190,
+ * the n_off_diag == 0 branch): the Feautrier system for u and for v (the
+ * same matrix, right-hand sides coupled through centred differences of the
+ * other term), elimination, back substitution to n_ar, diagonal ALO there. */
+static void solve_scattering(raypair_buf *b, const double *term2, double *Sv, int64_t ndep,
+                             int64_t n_ar, double I_bdy_0, double I_bdy_n, double *u, double *v,
+                             double *L)
+{
+    double *A = b->A, *C = b->C, *F = b->F, *G = b->G, *Su = b->Su, *dtau = b->dtau;
+    double *inv_A = b->inv_A, *inv_C = b->inv_C, *inv1pF = b->inv1pF, *GoG = b->GoG;
+    const double *term1 = b->term1;
+    const double inverse_dtau0 = 1.0 / dtau[0];
+    const double inverse_dtaud = 1.0 / dtau[ndep - 2];
+    C[0] = 2.0 * inverse_dtau0 * inverse_dtau0;
+    const double B0_min_C0 = 1.0 + 2.0 * inverse_dtau0;
+    const double B0 = B0_min_C0 + C[0];
+    const double inverse_B0 = 1.0 / B0;
+    Su[0] = term1[0] - (term2[1] + term2[0] - 2.0 * I_bdy_0) * inverse_dtau0;
+    Sv[0] = term2[0] - (term1[1] + term1[0] - 2.0 * I_bdy_0) * inverse_dtau0;
+    for (int64_t n = 1; n < ndep - 1; n++) {
+        inv_A[n] = 0.5 * (dtau[n - 1] + dtau[n]) * dtau[n - 1];
+        A[n] = 1.0 / inv_A[n];
+        inv_C[n] = 0.5 * (dtau[n - 1] + dtau[n]) * dtau[n];
+        C[n] = 1.0 / inv_C[n];
+        Su[n] = term1[n] - dtau[n] * C[n] * (term2[n + 1] - term2[n - 1]);
+        Sv[n] = term2[n] - dtau[n] * C[n] * (term1[n + 1] - term1[n - 1]);
+    }
+    A[ndep - 1] = 2.0 * inverse_dtaud * inverse_dtaud;
+    const double Bd_min_Ad = 1.0 + 2.0 * inverse_dtaud;
+    const double Bd = Bd_min_Ad + A[ndep - 1];
+    Su[ndep - 1] = term1[ndep - 1] + (term2[ndep - 1] + term2[ndep - 2] + 2.0 * I_bdy_n) * inverse_dtaud;
+    Sv[ndep - 1] = term2[ndep - 1] + (term1[ndep - 1] + term1[ndep - 2] - 2.0 * I_bdy_n) * inverse_dtaud;
+    Su[0] = Su[0] * inverse_B0;
+    Sv[0] = Sv[0] * inverse_B0;
+    F[0] = 0.5 * B0_min_C0 * dtau[0] * dtau[0];
+    inv1pF[0] = 1.0 / (1.0 + F[0]);
+    for (int64_t n = 1; n < ndep - 1; n++) {
+        F[n] = (1.0 + A[n] * F[n - 1] * inv1pF[n - 1]) * inv_C[n];
+        inv1pF[n] = 1.0 / (1.0 + F[n]);
+        Su[n] = (Su[n] + A[n] * Su[n - 1]) * inv1pF[n] * inv_C[n];
+        Sv[n] = (Sv[n] + A[n] * Sv[n - 1]) * inv1pF[n] * inv_C[n];
+    }
+    const double denominator = 1.0 / (Bd_min_Ad + Bd * F[ndep - 2]);
+    Su[ndep - 1] = (Su[ndep - 1] + A[ndep - 1] * Su[ndep - 2]) * (1.0 + F[ndep - 2]) * denominator;
+    Sv[ndep - 1] = (Sv[ndep - 1] + A[ndep - 1] * Sv[ndep - 2]) * (1.0 + F[ndep - 2]) * denominator;
+    if (n_ar < ndep - 1) {
+        G[ndep - 1] = 0.5 * Bd_min_Ad * dtau[ndep - 2] * dtau[ndep - 2];
+        GoG[ndep - 1] = G[ndep - 1] / (1.0 + G[ndep - 1]);
+        for (int64_t n = ndep - 2; n > n_ar; n--) {
+            Su[n] = Su[n] + Su[n + 1] * inv1pF[n];
+            Sv[n] = Sv[n] + Sv[n + 1] * inv1pF[n];
+            G[n] = (1.0 + C[n] * GoG[n + 1]) * inv_A[n];
+            GoG[n] = G[n] / (1.0 + G[n]);
+        }
+        Su[n_ar] = Su[n_ar] + Su[n_ar + 1] * inv1pF[n_ar];
+        Sv[n_ar] = Sv[n_ar] + Sv[n_ar + 1] * inv1pF[n_ar];
+        *L = inv_C[n_ar] / (F[n_ar] + GoG[n_ar + 1]);
+    } else {
+        *L = (1.0 + F[ndep - 2]) / (Bd_min_Ad + Bd * F[ndep - 2]);
+    }
+    *u = Su[n_ar];
+    *v = Sv[n_ar];
+}
+
+/* The formal solve with scattering terms: for every ray pair R < nrays/2 and
+ * origin, setup_using_scattering + solve_using_scattering at every bin, the
+ * J and ALO updates of compute_radiation_field (sim_radiation.tpp:150-264),
+ * and u, v at the origin per (R, o, f) as Radiation stores them
+ * (sim_radiation.tpp:226-236: u as is, v with its sign flipped when the ray
+ * r rather than its antipode is in front).  U, V, u_out, v_out:
+ * [nrays/2][ncells*nfreqs]. */
+int orc_compute_radiation_field_scattering(const orc_model *m, orc_state *s,
+                                           const int64_t *antipod, const double *U,
+                                           const double *V, double *u_out, double *v_out,
+                                           int nthreads)
+{
+    const int64_t nf = s->nfreqs, N = m->ncells, np = m->nrays / 2;
+    line_table lt;
+    lt.line = (double *)malloc(sizeof(double) * m->nrad);
+    lt.line_index = (int64_t *)malloc(sizeof(int64_t) * m->nrad);
+    sorted_lines(m, lt.line, lt.line_index);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    memset(s->J, 0, sizeof(double) * (size_t)(N * nf));
+    memset(s->Ls, 0, sizeof(double) * (size_t)(N * m->nrad));
+    int64_t errs = 0;
+    for (int64_t r = 0; r < np; r++) {
+        const int64_t ar = antipod[r];
+        const double weight_ang = m->ray_weights[r];
+#pragma omp parallel reduction(+ : errs)
+        {
+            trace_buf tr = {0, 0, NULL, NULL, NULL, 1, 0};
+            trace_buf ta = {0, 0, NULL, NULL, NULL, 1, 0};
+            raypair_buf rb;
+            memset(&rb, 0, sizeof(rb));
+            double *term2 = NULL, *Sv = NULL;
+            int64_t cap = 0;
+#pragma omp for schedule(static, 1)
+            for (int64_t o = 0; o < N; o++) {
+                const double dshift_max = orc_dshift_max(m, o);
+                int64_t e1 = 0, e2 = 0;
+                trace(m, o, r, dshift_max, &tr, &e1);
+                trace(m, o, ar, dshift_max, &ta, &e2);
+                if (e1 || e2) { errs++; continue; }
+                const int r_front = tr.n > ta.n;
+                const trace_buf *front = r_front ? &tr : &ta;
+                const trace_buf *back = r_front ? &ta : &tr;
+                const int64_t n_ar = front->n, ndep = front->n + back->n + 1;
+                if (ndep > 1) {
+                    rp_ensure(&rb, ndep + 1);
+                    if (ndep + 1 > cap) {
+                        cap = ndep + 64;
+                        term2 = (double *)realloc(term2, sizeof(double) * (size_t)cap);
+                        Sv = (double *)realloc(Sv, sizeof(double) * (size_t)cap);
+                    }
+                    int64_t lnotch_at_origin = 0;
+                    for (int64_t i = 0; i < ndep; i++) rb.notch[i] = 0;
+                    for (int64_t f = 0; f < nf; f++) {
+                        double I0, In, u, v, Ld;
+                        setup_scattering(m, s, &lt, o, f, r, U, V, front, back, &rb, term2,
+                                         &lnotch_at_origin, &I0, &In);
+                        solve_scattering(&rb, term2, Sv, ndep, n_ar, I0, In, &u, &v, &Ld);
+                        if (s->appears[f]) {
+                            const int64_t k = s->corr_k[f], z = s->corr_z[f];
+                            const double freq_line = m->frequency[k];
+                            const double weight = m->quad_weights[z] * 2.0 * weight_ang;
+                            const double factor = m->A[k] * weight;
+                            const double prof = profile(freq_line * profile_width(m, rb.nrs[n_ar]),
+                                                        rb.frs[n_ar] - freq_line);
+                            s->Ls[o * m->nrad + k] += factor * (rb.frs[n_ar] * prof * Ld / rb.chi[n_ar]);
+                        }
+                        s->J[o * nf + f] += 2.0 * weight_ang * u;
+                        u_out[r * N * nf + o * nf + f] = u;
+                        v_out[r * N * nf + o * nf + f] = r_front ? -v : v;
+                    }
+                } else {
+                    const int64_t b = m->cell2boundary[o];
+                    for (int64_t f = 0; f < nf; f++) {
+                        const double u = 0.5 * (s->I_bdy[b * nf + f] + s->I_bdy[b * nf + f]);
+                        const double v = 0.5 * (s->I_bdy[b * nf + f] - s->I_bdy[b * nf + f]);
+                        s->J[o * nf + f] += 2.0 * weight_ang * u;
+                        u_out[r * N * nf + o * nf + f] = u;
+                        v_out[r * N * nf + o * nf + f] = v;
+                    }
+                }
+            }
+            free(tr.cell); free(tr.shift); free(tr.dZ);
+            free(ta.cell); free(ta.shift); free(ta.dZ);
+            rp_free(&rb);
+            free(term2); free(Sv);
+        }
+    }
+    s->trace_errors = errs;
+    free(lt.line); free(lt.line_index);
+    return errs ? 1 : 0;
+}
+
+/* Radiation::calc_U_and_V (Model/Radiation/radiation.cpp:330-434, one
+ * process): the direction integrals U[r1] = sum over pairs r2 of u[r2] and
+ * V[r1] likewise (the phase function is 1), the same for every r1. */
+void orc_calc_U_and_V(const orc_model *m, const orc_state *s, const double *u, const double *v,
+                      double *U, double *V)
+{
+    const int64_t n = m->ncells * s->nfreqs, np = m->nrays / 2;
+    for (int64_t r1 = 0; r1 < np; r1++) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; i++) {
+            double su = 0.0, sv = 0.0;
+            for (int64_t r2 = 0; r2 < np; r2++) { su += u[r2 * n + i]; sv += v[r2 * n + i]; }
+            U[r1 * n + i] = su;
+            V[r1 * n + i] = sv;
+        }
+    }
+}
+
 /* ------------------------------------------------------------------ images */
 
 /* Simulation::compute_spectral_discretisation_image, Simulation/sim_spectrum.tpp:200-250:

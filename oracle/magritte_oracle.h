@@ -122,6 +122,12 @@ void orc_lte(const orc_model *m, orc_state *s);
 void orc_set_emissivity_opacity(const orc_model *m, orc_state *s);
 
 /* formal solve over all ray pairs (or a subset of origins / pairs) */
+int orc_compute_radiation_field_scattering(const orc_model *m, orc_state *s,
+                                           const int64_t *antipod, const double *U,
+                                           const double *V, double *u_out, double *v_out,
+                                           int nthreads);
+void orc_calc_U_and_V(const orc_model *m, const orc_state *s, const double *u, const double *v,
+                      double *U, double *V);
 int orc_image_discretisation(const orc_model *m, orc_state *s, double width);
 int orc_compute_image(const orc_model *m, orc_state *s, const int64_t *antipod, int64_t r,
                       double *I_m, double *I_p, int nthreads);

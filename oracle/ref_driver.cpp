@@ -14,6 +14,13 @@
 //                                              of every iteration
 //   magritte_ref <model/> <out/> trace <o...>  the traced points of every
 //                                              ray of the given origins
+//   magritte_ref <model/> <out/> scatter <U> <V>  every ray pair and origin
+//                                              through setup_using_scattering
+//                                              and solve_using_scattering with
+//                                              the scattering terms U, V read
+//                                              from raw files ([nrays/2]
+//                                              [ncells*nfreqs]): u, v at the
+//                                              origins and J (LTE populations)
 //   magritte_ref <model/> <out/> image <r> <w> compute_and_write_image along
 //                                              ray r on the image grid of
 //                                              relative width w (LTE
@@ -141,6 +148,64 @@ int main(int argc, char **argv) {
         write_raw_long(out + "/trace_cell.bin", cells);
         write_raw(out + "/trace_shift.bin", sh);
         write_raw(out + "/trace_dZ.bin", dz);
+        return 0;
+    }
+    if (cmd == "scatter" && argc > 5) {
+        set_up(sim, true);
+        const size_t N = sim.parameters.ncells(), nf = sim.parameters.nfreqs_red();
+        const size_t np = sim.parameters.nrays() / 2;
+        std::vector<double> U(np * N * nf), V(np * N * nf);
+        {
+            std::ifstream fu(argv[4], std::ios::binary), fv(argv[5], std::ios::binary);
+            fu.read(reinterpret_cast<char *>(U.data()), (std::streamsize)(U.size() * sizeof(double)));
+            fv.read(reinterpret_cast<char *>(V.data()), (std::streamsize)(V.size() * sizeof(double)));
+        }
+        sim.radiation.U.assign(np, std::vector<double>(N * nf));
+        sim.radiation.V.assign(np, std::vector<double>(N * nf));
+        for (size_t r = 0; r < np; r++)
+            for (size_t i = 0; i < N * nf; i++) {
+                sim.radiation.U[r][i] = U[r * N * nf + i];
+                sim.radiation.V[r][i] = V[r * N * nf + i];
+            }
+        sim.get_max_npoints_on_rays<CoMoving>();
+        RayPair rp;
+        rp.resize(sim.geometry.max_npoints_on_rays, 0);
+        std::vector<double> uo(np * N * nf), vo(np * N * nf), J(N * nf, 0.0);
+        for (size_t r = 0; r < np; r++) {
+            const long ar = sim.geometry.rays.antipod[r];
+            for (size_t o = 0; o < N; o++) {
+                const double w = sim.geometry.rays.weight(o, r);
+                const double dsm = sim.get_dshift_max(o);
+                RayData rd_r = sim.geometry.trace_ray<CoMoving>(o, r, dsm);
+                RayData rd_ar = sim.geometry.trace_ray<CoMoving>(o, ar, dsm);
+                const bool rf = rd_r.size() > rd_ar.size();
+                const size_t n_front = rf ? rd_r.size() : rd_ar.size();
+                const size_t n_back = rf ? rd_ar.size() : rd_r.size();
+                rp.initialize(n_front, n_back);
+                for (size_t f = 0; f < nf; f++) {
+                    double u, v;
+                    if (n_front + n_back + 1 > 1) {
+                        if (rf) sim.setup_using_scattering(r, o, f, rd_r, rd_ar, rp);
+                        else    sim.setup_using_scattering(r, o, f, rd_ar, rd_r, rp);
+                        rp.solve_using_scattering();
+                        u = rp.get_u_at_origin();
+                        v = rp.get_v_at_origin();
+                        if (rf) v = -v;
+                    } else {
+                        const long b = sim.geometry.boundary.cell2boundary_nr[o];
+                        const double I = sim.radiation.I_bdy[r][b][f];
+                        u = 0.5 * (I + I);
+                        v = 0.5 * (I - I);
+                    }
+                    J[o * nf + f] += 2.0 * w * u;
+                    uo[r * N * nf + o * nf + f] = u;
+                    vo[r * N * nf + o * nf + f] = v;
+                }
+            }
+        }
+        write_raw(out + "/u.bin", uo);
+        write_raw(out + "/v.bin", vo);
+        write_raw(out + "/J.bin", J);
         return 0;
     }
     if (cmd == "image" && argc > 5) {

@@ -199,6 +199,20 @@ def test_mixed_patches_inverted_lines(gpu):
     patched, fallbacks = sim.patch_stats()
     assert patched > 0 and fallbacks == 0
     assert rel_err(sim.J, J64, floor=1e-6 * np.abs(J64).max()) < MIXED_RTOL
+    # a patch list far too small: the origins whose failures overflow it are
+    # solved again in double, the rest keeps its float solve and patches
+    J_ok, L_ok = sim.J.copy(), sim.Lambda.copy()
+    sim.set_patch_capacity(16)
+    sim.compute_radiation_field("mixed", keep_J=True)
+    patched2, fallbacks2 = sim.patch_stats()
+    assert 0 < fallbacks2 < model.ncells
+    assert rel_err(sim.J, J64, floor=1e-6 * np.abs(J64).max()) < MIXED_RTOL
+    assert rel_err(sim.Lambda, L64, floor=1e-6 * np.abs(L64).max()) < MIXED_RTOL
+    # and through the traces rebuilt per batch of origins
+    sim.set_trace_budget(1 << 19)
+    sim.compute_radiation_field("mixed", keep_J=True)
+    assert rel_err(sim.J, J_ok, floor=1e-6 * np.abs(J64).max()) < MIXED_RTOL
+    assert rel_err(sim.Lambda, L_ok, floor=1e-6 * np.abs(L64).max()) < MIXED_RTOL
 
 
 def test_generic_kernels_few_bins(gpu):

@@ -226,3 +226,55 @@ def test_image_matches_reference(tmp_path, make, ray, width):
     d = str(out) + "/"
     assert rel(I_m, io_text.read_array(d, f"Simulation/Image/I_m_{ray}")) <= 1e-12
     assert rel(I_p, io_text.read_array(d, f"Simulation/Image/I_p_{ray}")) <= 1e-12
+
+
+def scattering_terms(model, orc):
+    """Deterministic U, V of emissivity size (the reference adds U to the
+    emissivity): fractions of the line emissivity at each cell's bins,
+    varying with pair, cell and bin."""
+    KB, AMU, CC = 1.38064852e-23, 1.66053904e-27, 2.99792458e8
+    pw = np.sqrt(2.0 * KB / (AMU * CC ** 2) * model.linedata.inverse_mass * model.temperature
+                 + model.vturb2)
+    nu = orc.nu
+    line = model.linedata.frequency
+    width = line[None, :] * pw[:, None]
+    x = (nu[:, :, None] - line[None, None, :]) / width[:, None, :]
+    phi = np.where(np.abs(x) <= 11.0, np.exp(-x * x) / (np.sqrt(np.pi) * width[:, None, :]), 0.0)
+    eta = (orc.emissivity[:, None, :] * nu[:, :, None] * phi).sum(-1)
+    np_, N, nf = model.nrays // 2, model.ncells, model.nfreqs
+    r = np.arange(np_)[:, None, None]
+    p = np.arange(N)[None, :, None]
+    f = np.arange(nf)[None, None, :]
+    U = eta[None] * (0.3 + 0.05 * r) * (1.0 + 0.2 * np.sin(0.37 * p + 0.11 * f))
+    V = eta[None] * 0.1 * np.cos(0.23 * p + 0.07 * f + 0.5 * r)
+    # zero beyond 3 Doppler widths of each line: rescale_U_and_V holds the
+    # edge value beyond a cell's grid, where the opacity that U is divided
+    # by falls to its 1e-26 floor
+    outer = np.tile(np.abs(model.quad_roots) >= 3.0, model.nlines)
+    U[:, :, outer] = 0.0
+    V[:, :, outer] = 0.0
+    return np.ascontiguousarray(U), np.ascontiguousarray(V)
+
+
+@needs_ref
+@pytest.mark.parametrize("make", [M.config1, small_wind])
+def test_scattering_solve_matches_reference(tmp_path, make):
+    """setup_using_scattering + solve_using_scattering (never called by the
+    reference's own driver) for every ray pair and origin, against the
+    oracle's restatement: u and v at the origins and J."""
+    model = make()
+    orc = oracle.Oracle(model).setup()
+    U, V = scattering_terms(model, orc)
+    U.tofile(str(tmp_path / "U.bin"))
+    V.tofile(str(tmp_path / "V.bin"))
+    out = run_ref(model, tmp_path, "scatter", str(tmp_path / "U.bin"), str(tmp_path / "V.bin"))
+    u, v = orc.compute_radiation_field_scattering(U, V, nthreads=THREADS)
+    shape = u.shape
+    ur = np.fromfile(out / "u.bin").reshape(shape)
+    vr = np.fromfile(out / "v.bin").reshape(shape)
+    assert rel(u, ur) <= 1e-12
+    nz = vr != 0
+    assert np.array_equal(v == 0, ~nz)
+    assert rel(v[nz], vr[nz]) <= 1e-12
+    J = np.fromfile(out / "J.bin").reshape(model.ncells, model.nfreqs)
+    assert rel(orc.J, J) <= 1e-12
