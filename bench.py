@@ -21,9 +21,10 @@ solve from LTE is measured in the same run and reported beside it.
            sample of origins, extrapolated, plus the full rate-equation step,
            times the iteration count of the solve
 
-``--impl reference`` times the CPU oracle (the reference's algorithm
-restated in C, OpenMP over origins as the reference does) the same way and
-prints one line with "impl": "reference".
+``--impl reference`` times the reference's own C++ (Magritte's CPU path
+compiled from its sources into oracle/_ref; the CPU oracle, the same
+algorithm restated in C, where that binary is absent) with OpenMP on every
+host core, and prints one line with "impl": "reference".
 
 Multi-GPU (torchrun): the ranks partition the origins of the one model
 (``magritte_b200.partition``: each rank solves its own origins and cells,
@@ -82,6 +83,8 @@ def parse():
                     help="with several GPUs, solve an independent replica per GPU instead of "
                          "partitioning one model")
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--ref-sample-s", type=float, default=3.0,
+                    help="seconds of the reference's formal-solve sample per step (reference arm)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -273,6 +276,58 @@ class CpuOracle:
                 "sample_origins": int(len(origins)), "cores": self.nthreads}
 
 
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "magritte_ref")
+
+
+class ReferenceCpu:
+    """The reference's own C++ (Magritte's CPU path compiled from its
+    sources into oracle/_ref, OpenMP on all host cores), fed the workload
+    as a model folder in its text layout.  A step times the reference's
+    per-origin work of compute_radiation_field (trace, setup, solve,
+    update_Lambda, J; sim_radiation.tpp:150-264) on a seeded sample of
+    origins over all ray pairs, scaled to every origin, times the number of
+    formal solves, plus the whole model's Jeff + rate-equation step per
+    formal solve and Ng step per Ng iteration (those two timed once per
+    run, on the full model)."""
+
+    def __init__(self, model, name, nthreads=None):
+        import tempfile
+        from magritte_b200 import io_text
+        self.model = model
+        self.nthreads = nthreads or os.cpu_count() or 1
+        self.dir = tempfile.mkdtemp(prefix=f"mgr_ref_{name}_")
+        self.folder = os.path.join(self.dir, "model") + "/"
+        io_text.write_model(model, self.folder)
+
+    def run(self, samples):
+        path = os.path.join(self.dir, "samples.txt")
+        with open(path, "w") as f:
+            for o in samples:
+                f.write(" ".join(str(int(x)) for x in o) + "\n")
+        env = dict(os.environ, OMP_NUM_THREADS=str(self.nthreads))
+        r = subprocess.run([REF_BIN, self.folder, self.dir, "sample", path], capture_output=True,
+                           text=True, env=env, cwd=self.dir)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr[-2000:])
+        return [json.loads(l) for l in r.stdout.splitlines() if l.startswith('{"origins"')]
+
+    def time_steps(self, n_solve, n_ng, sample_s, steps, seed0=0):
+        import numpy as np
+        N = self.model.ncells
+        rng = np.random.default_rng(seed0)
+        probe = self.run([np.sort(rng.choice(N, size=min(256, N), replace=False))])[0]
+        per_origin = probe["formal_solve_s"] / probe["origins"]
+        n = int(min(N, max(64, sample_s / max(per_origin, 1e-9))))
+        samples = [np.sort(rng.choice(N, size=n, replace=False)) for _ in range(steps)]
+        out = self.run(samples)
+        t_stateq, t_ng = probe["stateq_s"], probe["ng_s"]
+        secs = [o["formal_solve_s"] * N / o["origins"] * n_solve + t_stateq * n_solve + t_ng * n_ng
+                for o in out]
+        info = {"sample_origins": n, "cores": self.nthreads, "stateq_s": t_stateq, "ng_s": t_ng,
+                "formal_solve_s": statistics.mean(o["formal_solve_s"] * N / o["origins"] for o in out)}
+        return secs, info
+
+
 def cpu_oracle_time(model, iterations, sample_s, nthreads=None):
     """The oracle's time for `iterations` iterations of the ALI loop, Ng
     steps (every fifth iteration) charged as Ng steps, not formal solves."""
@@ -321,14 +376,31 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           f"no measured iteration count of the oracle for {args.workload}"}))
         return
-    cpu = CpuOracle(model)
-    for w in range(args.warmup):
-        cpu.time(n_solve, min(2.0, args.cpu_sample_s), seed=100 + w, ng_steps=n_ng)
-    steps = []
-    info = None
-    for k in range(max(1, args.steps)):
-        info = cpu.time(n_solve, args.cpu_sample_s, seed=k, ng_steps=n_ng)
-        steps.append(info["seconds"])
+    if os.path.exists(REF_BIN):
+        # the reference's own compiled C++; warm-up samples lead the run
+        ref = ReferenceCpu(model, args.workload)
+        secs, info = ref.time_steps(n_solve, n_ng, args.ref_sample_s,
+                                    args.warmup + max(1, args.steps))
+        steps = secs[args.warmup:]
+        kind = "reference"
+        sample = (f"the reference's compiled per-origin work of compute_radiation_field over "
+                  f"{info['sample_origins']} seeded origins x all ray pairs per step, scaled to "
+                  f"{model.ncells} origins, x {n_solve} formal solves; plus its full-model Jeff + "
+                  f"rate-equation step ({info['stateq_s']:.2f} s, x {n_solve}) and Ng step "
+                  f"({info['ng_s']:.2f} s, x {n_ng}), timed once")
+    else:
+        cpu = CpuOracle(model)
+        for w in range(args.warmup):
+            cpu.time(n_solve, min(2.0, args.cpu_sample_s), seed=100 + w, ng_steps=n_ng)
+        steps = []
+        info = None
+        for k in range(max(1, args.steps)):
+            info = cpu.time(n_solve, args.cpu_sample_s, seed=k, ng_steps=n_ng)
+            steps.append(info["seconds"])
+        kind = "port"
+        sample = (f"one formal solve over {info['sample_origins']} seeded origins x all ray pairs "
+                  f"scaled to {model.ncells} origins, plus one full Jeff + rate-equation step, x "
+                  f"{n_solve} formal solves; plus {n_ng} full Ng step(s)")
     value = statistics.mean(steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s",
@@ -338,12 +410,8 @@ def run_reference(args):
         "config": workload_config(args.workload, model, "fp64"),
         "ali_iterations": n_solve + n_ng, "formal_solves": n_solve, "ng_steps": n_ng,
         "iteration_source": source,
-        "cpu_baseline": {"value": value, "unit": "s", "cores": info["cores"], "kind": "port",
-                         "cpu_model": cpu_model(),
-                         "sample": f"one formal solve over {info['sample_origins']} seeded origins "
-                                   f"x all ray pairs scaled to {model.ncells} origins, plus one "
-                                   f"full Jeff + rate-equation step, x {n_solve} formal solves; "
-                                   f"plus {n_ng} full Ng step(s)"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": info["cores"], "kind": kind,
+                         "cpu_model": cpu_model(), "sample": sample},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -466,7 +534,7 @@ def run_b200(args):
             sim.compute_radiation_field("fp64")
     if dist:
         tdist.barrier()
-    times, iters, solve_ms, solve_upd = [], [], [], []
+    times, iters, solve_ms, solve_upd, trace_ms = [], [], [], [], []
     with Clocks(local) as clk:
         time.sleep(2.0)          # sampler start-up outside the timed steps
         if args.warmup > 0:
@@ -483,6 +551,7 @@ def run_b200(args):
             ms, up = sim.solve_stats()
             solve_ms.append(ms)
             solve_upd.append(up)
+            trace_ms.append(sim.solve_trace_ms())
         clk.mark_end()
     launches = (sim.launch_count() - launches0) // max(1, args.steps)
     converged = bool(getattr(sim, "converged", False))
@@ -589,7 +658,11 @@ def run_b200(args):
         "plain_fp64_lte": plain,
         "final_max_rel_change": err_hist[-1] if err_hist else None,
         "formal_solve": {"ms": avg_ms, "updates": solve_upd[-1],
-                         "updates_per_s": solve_upd[-1] / (avg_ms / 1e3)},
+                         "updates_per_s": solve_upd[-1] / (avg_ms / 1e3),
+                         "trace_rebuild_ms": statistics.mean(trace_ms),
+                         "note": "ms of the last formal solve of each step; trace_rebuild_ms: of "
+                                 "it, rebuilding the traces batch by batch of origins when they "
+                                 "exceed the trace budget (0: traces stored)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic,
                      "note": f"formal-solve kernel; effective operand bytes {bpu:.0f} B/update "
@@ -604,14 +677,29 @@ def run_b200(args):
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline and world == 1:
-        info = cpu_oracle_time(model, iters[-1], args.cpu_sample_s)
-        line["cpu_baseline"] = {
-            "value": info["seconds"], "unit": "s", "cores": info["cores"], "kind": "port",
-            "cpu_model": cpu_model(),
-            "sample": f"one formal solve over {info['sample_origins']} seeded origins x all ray "
-                      f"pairs scaled to {model.ncells} origins, plus one full Jeff + "
-                      f"rate-equation step, x {info['formal_solves']} formal solves, plus "
-                      f"{info['ng_steps']} full Ng step(s) ({iters[-1]} iterations)"}
+        from oracle.measure_iterations import step_kinds
+        k = step_kinds(iters[-1])
+        n_solve, n_ng = k.count("solve"), k.count("ng")
+        if os.path.exists(REF_BIN):
+            secs, info = ReferenceCpu(model, args.workload).time_steps(n_solve, n_ng,
+                                                                     args.cpu_sample_s, 1)
+            line["cpu_baseline"] = {
+                "value": secs[0], "unit": "s", "cores": info["cores"], "kind": "reference",
+                "cpu_model": cpu_model(),
+                "sample": f"the reference's compiled per-origin work of compute_radiation_field "
+                          f"over {info['sample_origins']} seeded origins x all ray pairs, scaled "
+                          f"to {model.ncells} origins, x {n_solve} formal solves, plus its "
+                          f"full-model Jeff + rate-equation and Ng steps ({iters[-1]} iterations "
+                          f"of the headline arm)"}
+        else:
+            info = cpu_oracle_time(model, iters[-1], args.cpu_sample_s)
+            line["cpu_baseline"] = {
+                "value": info["seconds"], "unit": "s", "cores": info["cores"], "kind": "port",
+                "cpu_model": cpu_model(),
+                "sample": f"one formal solve over {info['sample_origins']} seeded origins x all "
+                          f"ray pairs scaled to {model.ncells} origins, plus one full Jeff + "
+                          f"rate-equation step, x {info['formal_solves']} formal solves, plus "
+                          f"{info['ng_steps']} full Ng step(s) ({iters[-1]} iterations)"}
     print(json.dumps(line), flush=True)
 
 

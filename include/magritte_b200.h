@@ -237,6 +237,11 @@ mgr_status mgr_get_frequencies(mgr_handle *h, double *nu);            /* [ncells
  * stream) and the ray-point-frequency updates it did. */
 mgr_status mgr_get_solve_stats(mgr_handle *h, double *ms, double *updates);
 
+/* Of the last formal solve's device time: the milliseconds spent
+ * rebuilding traces, batch by batch of origins, when the traces exceed the
+ * trace budget (0 when they are stored).  No reference counterpart. */
+mgr_status mgr_get_solve_breakdown(mgr_handle *h, double *trace_ms);
+
 /* Mixed precision: (origin, pair, bin) solves of the last formal solve that
  * were redone in double (inverted lines driving the opacity below half its
  * 1e-26 floor, or a float failure), and the number of origins since

@@ -42,7 +42,7 @@ EXPORTS = (
     "mgr_get_device_buffer", "mgr_get_population_history", "mgr_set_population_history",
     "mgr_compute_image", "mgr_set_patch_capacity", "mgr_set_scattering_terms",
     "mgr_get_scattering_terms", "mgr_compute_radiation_field_scattering", "mgr_get_scattering_uv",
-    "mgr_calc_U_and_V",
+    "mgr_calc_U_and_V", "mgr_get_solve_breakdown",
 )
 # mgr_buffer
 BUF_POPULATION, BUF_PREV1, BUF_PREV2, BUF_PREV3, BUF_JLIN, BUF_LAMBDA, BUF_PARTIALS = range(7)
@@ -157,6 +157,7 @@ def load(build_if_missing: bool = True):
     L.mgr_compute_radiation_field_scattering.argtypes = [_P]
     L.mgr_get_scattering_uv.argtypes = [_P, _P, _P]
     L.mgr_calc_U_and_V.argtypes = [_P]
+    L.mgr_get_solve_breakdown.argtypes = [_P, C.POINTER(_dbl)]
     L.mgr_set_population_history.argtypes = [_P, _P, _P, _P, _P]
     L.mgr_mlp_param_count.argtypes = [_i32, C.POINTER(_i64)]
     L.mgr_get_features.argtypes = [_P, _P]

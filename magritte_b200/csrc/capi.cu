@@ -97,6 +97,8 @@ struct mgr_handle {
     bool model_loaded = false, line_set = false, bdy_set = false, pops_valid = false;
     bool keep_J = false;
     double last_solve_ms = 0.0, last_updates = 0.0;
+    double last_trace_ms = 0.0;        // of the last solve: rebuilding traces per batch of origins
+    std::vector<cudaEvent_t> batch_ev; // [2 per batch] around each batch's trace rebuild
 
     std::vector<int64_t> antipod;
     int64_t nboundary = 0;
@@ -913,6 +915,7 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
         ck(cudaStreamSynchronize(h->stream), "solve sync");
         finish_solve(h, precision, variant, timing,
                      precision == MGR_MIXED ? (int64_t)*h->h_patch : 0);
+        h->last_trace_ms = 0.0;
         return;
     }
     // traces in batches of origins, rebuilt for every solve
@@ -921,9 +924,18 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
     unsigned long long patched = 0;
     int64_t redo_done = 0;
     ck(cudaEventRecord(h->ev0, h->stream), "event");
-    for (int64_t o0 = h->o_begin; o0 < h->o_end; o0 += h->batch_origins) {
+    const int64_t nbatches = (h->o_end - h->o_begin + h->batch_origins - 1) / h->batch_origins;
+    while ((int64_t)h->batch_ev.size() < 2 * nbatches) {
+        cudaEvent_t e;
+        ck(cudaEventCreate(&e), "event");
+        h->batch_ev.push_back(e);
+    }
+    int64_t bi = 0;
+    for (int64_t o0 = h->o_begin; o0 < h->o_end; o0 += h->batch_origins, bi++) {
         const int64_t cnt = std::min(h->batch_origins, h->o_end - o0);
+        ck(cudaEventRecord(h->batch_ev[2 * bi], h->stream), "event");
         TraceView t = build_batch(h, o0, cnt);
+        ck(cudaEventRecord(h->batch_ev[2 * bi + 1], h->stream), "event");
         SolveArgs ab = a;   // a batch's store holds exactly the origins it solves
         ab.s_begin = 0;
         ab.s_end = cnt;
@@ -954,7 +966,14 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
     ck(cudaEventRecord(h->ev1, h->stream), "event");
     ck(cudaMemcpyAsync(h->h_flags, h->flags, sizeof(DevFlags), cudaMemcpyDeviceToHost, h->stream), "flags");
     ck(cudaStreamSynchronize(h->stream), "solve sync");
+    double trace_ms = 0.0;
+    for (int64_t b = 0; b < bi; b++) {
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, h->batch_ev[2 * b], h->batch_ev[2 * b + 1]), "elapsed");
+        trace_ms += ms;
+    }
     finish_solve(h, precision, variant, timing, (int64_t)patched);
+    h->last_trace_ms = trace_ms;
 }
 
 void read_stats(mgr_handle *h) {
@@ -1091,6 +1110,7 @@ mgr_status mgr_destroy(mgr_handle *h) {
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->tev0) cudaEventDestroy(h->tev0);
     if (h->tev1) cudaEventDestroy(h->tev1);
+    for (cudaEvent_t e : h->batch_ev) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return MGR_OK;
@@ -1560,6 +1580,12 @@ mgr_status mgr_set_patch_capacity(mgr_handle *h, int64_t entries) {
         free_ptr((void *&)h->redo_list);
         h->patch_cap_set = entries;
         h->gen++;
+    });
+}
+
+mgr_status mgr_get_solve_breakdown(mgr_handle *h, double *trace_ms) {
+    return run(h, [&] {
+        if (trace_ms) *trace_ms = h->last_trace_ms;
     });
 }
 

@@ -659,8 +659,21 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
         }
         s = 2;
     }
-    // both halves
+    // both halves: four steps between renormalisations (b shrinks by at
+    // most dh^2 per step, dh >= ~5e-20 on floor-opacity sub-points, so four
+    // steps stay far inside the double range)
     const int e1 = min(s1, nbk);
+    for (; s + 3 < e1; s += 4) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            staged_eval<kCheck>(F + s + j, eo, q, floor_hat, chi, t_);
+            staged_eval<kCheck>(B + s + j, eo, q, floor_hat, chi2, t2);
+            fr.step(chi, t_, F[s + j].dzh);
+            bk.step(chi2, t2, B[s + j].dzh);
+        }
+        fr.renorm();
+        bk.renorm();
+    }
     for (; s + 1 < e1; s += 2) {
         staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
         staged_eval<kCheck>(B + s, eo, q, floor_hat, chi2, t2);
@@ -683,6 +696,14 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
         s++;
     }
     // the rest of the front half
+    for (; s + 3 < s1; s += 4) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            staged_eval<kCheck>(F + s + j, eo, q, floor_hat, chi, t_);
+            fr.step(chi, t_, F[s + j].dzh);
+        }
+        fr.renorm();
+    }
     for (; s + 1 < s1; s += 2) {
         staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
         fr.step(chi, t_, F[s].dzh);
@@ -833,6 +854,17 @@ __device__ __forceinline__ void staged_window64(const StagedPt64 *F, const Stage
         s = 2;
     }
     const int e1 = min(s1, nbk);
+    for (; s + 3 < e1; s += 4) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            staged_eval64(F + s + j, ln, chi, t_);
+            staged_eval64(B + s + j, ln, chi2, t2);
+            fr.step(chi, t_, F[s + j].dzq);
+            bk.step(chi2, t2, B[s + j].dzq);
+        }
+        fr.renorm();
+        bk.renorm();
+    }
     for (; s + 1 < e1; s += 2) {
         staged_eval64(F + s, ln, chi, t_);
         staged_eval64(B + s, ln, chi2, t2);
@@ -853,6 +885,14 @@ __device__ __forceinline__ void staged_window64(const StagedPt64 *F, const Stage
         fr.renorm();
         bk.renorm();
         s++;
+    }
+    for (; s + 3 < s1; s += 4) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            staged_eval64(F + s + j, ln, chi, t_);
+            fr.step(chi, t_, F[s + j].dzq);
+        }
+        fr.renorm();
     }
     for (; s + 1 < s1; s += 2) {
         staged_eval64(F + s, ln, chi, t_);

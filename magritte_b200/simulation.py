@@ -375,6 +375,13 @@ class Simulation:
         d = net.desc()
         return self._ck(self._lib.mgr_warm_start(self._h, C.byref(d)))
 
+    def solve_trace_ms(self) -> float:
+        """Of the last formal solve: ms spent rebuilding traces per batch of
+        origins (0 when the traces are stored)."""
+        t = C.c_double()
+        self._ck(self._lib.mgr_get_solve_breakdown(self._h, C.byref(t)))
+        return t.value
+
     def solve_stats(self):
         ms, up = C.c_double(), C.c_double()
         self._ck(self._lib.mgr_get_solve_stats(self._h, C.byref(ms), C.byref(up)))

@@ -68,3 +68,16 @@ compile -c "$HERE/ref_driver.cpp" -o "$OUT/obj/ref_driver.o" &
 while [ "$(jobs -rp | wc -l)" -gt 0 ]; do wait -n; done
 "$CXX" -fopenmp -o "$OUT/magritte_ref" "${objs[@]}" "$OUT/obj/raypair_fixed.o" "$OUT/obj/ref_driver.o"
 echo "$OUT/magritte_ref"
+
+# Magritte's Simulation routed to the B200 library through the C++ binding
+# of magritte_b200/integration (needs libmagritte_b200.so built first)
+LIBDIR="$(cd "$HERE/.." && pwd)/magritte_b200"
+if [ -f "$LIBDIR/libmagritte_b200.so" ]; then
+    INC=(-I "$(cd "$HERE/.." && pwd)/include" -I "$LIBDIR/integration")
+    compile "${INC[@]}" -c "$LIBDIR/integration/magritte_b200_binding.cpp" -o "$OUT/obj/binding.o"
+    compile "${INC[@]}" -c "$HERE/ref_b200_driver.cpp" -o "$OUT/obj/ref_b200_driver.o"
+    "$CXX" -fopenmp -o "$OUT/magritte_ref_b200" "${objs[@]}" "$OUT/obj/raypair_fixed.o" \
+        "$OUT/obj/binding.o" "$OUT/obj/ref_b200_driver.o" -L "$LIBDIR" -lmagritte_b200 \
+        -Wl,-rpath,'$ORIGIN/../../magritte_b200'
+    echo "$OUT/magritte_ref_b200"
+fi

@@ -14,6 +14,16 @@
 //                                              of every iteration
 //   magritte_ref <model/> <out/> trace <o...>  the traced points of every
 //                                              ray of the given origins
+//   magritte_ref <model/> <out/> sample <file>  timing of the reference's own
+//                                              per-origin work of
+//                                              compute_radiation_field (the
+//                                              body of its loop, sim_radiation.
+//                                              tpp:150-264) over each line's
+//                                              origins, OpenMP over origins as
+//                                              there, one JSON line per sample;
+//                                              after the first sample also one
+//                                              full Jeff + statistical-
+//                                              equilibrium step and one Ng step
 //   magritte_ref <model/> <out/> scatter <U> <V>  every ray pair and origin
 //                                              through setup_using_scattering
 //                                              and solve_using_scattering with
@@ -32,11 +42,14 @@
 // compute_boundary_intensities, compute_LTE_level_populations, ...), with
 // the boundary temperatures of the model folder passed to
 // compute_boundary_intensities (sim_radiation.tpp:17-40).
+#include <omp.h>
 #include <sys/stat.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -148,6 +161,79 @@ int main(int argc, char **argv) {
         write_raw_long(out + "/trace_cell.bin", cells);
         write_raw(out + "/trace_shift.bin", sh);
         write_raw(out + "/trace_dZ.bin", dz);
+        return 0;
+    }
+    if (cmd == "sample" && argc > 4) {
+        set_up(sim, true);
+        sim.get_max_npoints_on_rays<CoMoving>();
+        const int nthr = omp_get_max_threads();
+        std::vector<RayPair> pairs(nthr);
+        for (auto &rp : pairs) rp.resize(sim.geometry.max_npoints_on_rays, sim.parameters.n_off_diag);
+        const size_t nf = sim.parameters.nfreqs_red();
+        const auto sec = [](std::chrono::steady_clock::time_point a,
+                            std::chrono::steady_clock::time_point b) {
+            return std::chrono::duration<double>(b - a).count();
+        };
+        std::ifstream lists(argv[4]);
+        std::string line;
+        bool first = true;
+        while (std::getline(lists, line)) {
+            std::vector<long> origins;
+            std::stringstream ss(line);
+            long o;
+            while (ss >> o) origins.push_back(o);
+            if (origins.empty()) continue;
+            for (LineProducingSpecies &lspec : sim.lines.lineProducingSpecies) lspec.lambda.clear();
+            sim.radiation.initialize_J();
+            const auto t0 = std::chrono::steady_clock::now();
+            for (size_t r = 0; r < sim.parameters.nrays() / 2; r++) {
+                const long R = (long)r;
+                const long ar = sim.geometry.rays.antipod[r];
+#pragma omp parallel for schedule(static, 1)
+                for (long i = 0; i < (long)origins.size(); i++) {
+                    RayPair &rp = pairs[omp_get_thread_num()];
+                    const long oo = origins[i];
+                    const double w = sim.geometry.rays.weight(oo, r);
+                    const double dsm = sim.get_dshift_max(oo);
+                    RayData rd_r = sim.geometry.trace_ray<CoMoving>(oo, r, dsm);
+                    RayData rd_ar = sim.geometry.trace_ray<CoMoving>(oo, ar, dsm);
+                    const bool rf = rd_r.size() > rd_ar.size();
+                    if (rf) rp.initialize(rd_r.size(), rd_ar.size());
+                    else    rp.initialize(rd_ar.size(), rd_r.size());
+                    if (rp.ndep > 1) {
+                        for (size_t f = 0; f < nf; f++) {
+                            if (rf) sim.setup(R, oo, f, rd_r, rd_ar, rp);
+                            else    sim.setup(R, oo, f, rd_ar, rd_r, rp);
+                            rp.solve();
+                            rp.update_Lambda(sim.radiation.frequencies, sim.thermodynamics, oo, f, w,
+                                             sim.lines);
+                            sim.radiation.J[sim.radiation.index(oo, f)] += 2.0 * w * rp.get_u_at_origin();
+                        }
+                    } else {
+                        const long b = sim.geometry.boundary.cell2boundary_nr[oo];
+                        for (size_t f = 0; f < nf; f++)
+                            sim.radiation.J[sim.radiation.index(oo, f)] +=
+                                2.0 * w * 0.5 * (sim.radiation.I_bdy[R][b][f] + sim.radiation.I_bdy[R][b][f]);
+                    }
+                }
+            }
+            const auto t1 = std::chrono::steady_clock::now();
+            double stateq_s = -1.0, ng_s = -1.0;
+            if (first) {   // the whole model's rate equations and Ng step, once
+                sim.compute_Jeff();
+                sim.compute_level_populations_from_stateq();
+                const auto t2 = std::chrono::steady_clock::now();
+                sim.lines.iteration_using_Ng_acceleration(sim.parameters.pop_prec());
+                const auto t3 = std::chrono::steady_clock::now();
+                stateq_s = sec(t1, t2);
+                ng_s = sec(t2, t3);
+                first = false;
+            }
+            std::printf("{\"origins\": %zu, \"threads\": %d, \"formal_solve_s\": %.6f, "
+                        "\"stateq_s\": %.6f, \"ng_s\": %.6f}\n",
+                        origins.size(), nthr, sec(t0, t1), stateq_s, ng_s);
+            std::fflush(stdout);
+        }
         return 0;
     }
     if (cmd == "scatter" && argc > 5) {
