@@ -93,9 +93,11 @@ def test_scattering_solve_matches_oracle(gpu, make):
     # small values to 1e-12 of the flux scale
     assert rel_err(u, u_o, floor=1e-9 * np.abs(u_o).max()) < FP64_RTOL
     assert rel_err(v, v_o, floor=1e-6 * np.abs(v_o).max()) < FP64_RTOL
-    assert rel_err(sim.J, orc.J) < FP64_RTOL
-    assert rel_err(sim.Jlin, orc.Jlin) < FP64_RTOL
-    assert rel_err(sim.Lambda, orc.Ls) < FP64_RTOL
+    # the scattering terms can drive J of the weakest lines slightly
+    # negative: the same floor of 1e-9 of the largest value
+    assert rel_err(sim.J, orc.J, floor=1e-9 * np.abs(orc.J).max()) < FP64_RTOL
+    assert rel_err(sim.Jlin, orc.Jlin, floor=1e-9 * np.abs(orc.Jlin).max()) < FP64_RTOL
+    assert rel_err(sim.Lambda, orc.Ls, floor=1e-9 * np.abs(orc.Ls).max()) < FP64_RTOL
     # the next scattering terms from this solve, and one more solve with them
     sim.calc_U_and_V()
     U2, V2 = sim.scattering_terms()
