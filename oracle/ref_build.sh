@@ -69,6 +69,41 @@ while [ "$(jobs -rp | wc -l)" -gt 0 ]; do wait -n; done
 "$CXX" -fopenmp -o "$OUT/magritte_ref" "${objs[@]}" "$OUT/obj/raypair_fixed.o" "$OUT/obj/ref_driver.o"
 echo "$OUT/magritte_ref"
 
+# The reference's GPU solver (Simulation::gpu_compute_radiation_field,
+# src/Simulation/simulation.cu, src/Simulation/Solver/gpu/gpu_solver.cu) in a
+# second build of the same sources with GPU_ACCELERATION on, as the
+# reference's CMake build makes it (src/CMakeLists.txt:50-88): the C++ units
+# by the host compiler, the two .cu units by nvcc with the reference's own
+# CUDA_NVCC_FLAGS "-O5 -use_fast_math" (CMakeLists.txt:20), for sm_100a.
+if command -v nvcc > /dev/null 2>&1; then
+    CUDA_HOME="${CUDA_HOME:-$(dirname "$(dirname "$(command -v nvcc)")")}"
+    mkdir -p "$OUT/obj_gpu"
+    GFLAGS=(-DMGR_REF_GPU -I "$CUDA_HOME/include")
+    gobjs=()
+    jobs_running=0
+    for u in "${UNITS[@]}"; do
+        o="$OUT/obj_gpu/$(echo "$u" | tr / _).o"
+        gobjs+=("$o")
+        compile "${GFLAGS[@]}" -c "$SRC/$u" -o "$o" &
+        jobs_running=$((jobs_running + 1))
+        if [ "$jobs_running" -ge 6 ]; then wait -n; jobs_running=$((jobs_running - 1)); fi
+    done
+    compile "${GFLAGS[@]}" -I "$SRC/Simulation/Raypair" -c "$OUT/raypair_fixed.cpp" \
+        -o "$OUT/obj_gpu/raypair_fixed.o" &
+    compile "${GFLAGS[@]}" -c "$HERE/ref_driver.cpp" -o "$OUT/obj_gpu/ref_driver.o" &
+    for u in Simulation/simulation.cu Simulation/Solver/gpu/gpu_solver.cu; do
+        o="$OUT/obj_gpu/$(echo "$u" | tr / _).o"
+        gobjs+=("$o")
+        nvcc -std=c++14 -O5 -use_fast_math -gencode arch=compute_100a,code=sm_100a -w \
+            -Xcompiler -fopenmp -DMGR_REF_GPU -I "$HERE/ref_shim" -I "$SRC" -I "$REF/dependencies" \
+            -c "$SRC/$u" -o "$o" &
+    done
+    while [ "$(jobs -rp | wc -l)" -gt 0 ]; do wait -n; done
+    "$CXX" -fopenmp -o "$OUT/magritte_ref_gpu" "${gobjs[@]}" "$OUT/obj_gpu/raypair_fixed.o" \
+        "$OUT/obj_gpu/ref_driver.o" -L "$CUDA_HOME/lib64" -lcudart -Wl,-rpath,"$CUDA_HOME/lib64"
+    echo "$OUT/magritte_ref_gpu"
+fi
+
 # Magritte's Simulation routed to the B200 library through the C++ binding
 # of magritte_b200/integration (needs libmagritte_b200.so built first)
 LIBDIR="$(cd "$HERE/.." && pwd)/magritte_b200"

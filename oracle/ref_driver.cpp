@@ -36,6 +36,14 @@
 //                                              relative width w (LTE
 //                                              populations): written by the
 //                                              reference's Image::write
+//   magritte_ref_gpu <model/> <out/> gpu <block> <nblocks> <reps>
+//                                              (the build with the
+//                                              reference's GPU solver only)
+//                                              gpu_compute_radiation_field
+//                                              with that launch shape, reps
+//                                              times, one JSON line of wall
+//                                              time each; then J, Jlin, Jeff,
+//                                              ALO as for radiation
 //
 // The call sequence follows the reference's examples
 // (src/examples/example_1.cpp: read, compute_spectral_discretisation,
@@ -303,6 +311,42 @@ int main(int argc, char **argv) {
         IoText io_out(out + "/");
         return sim.compute_and_write_image(io_out, std::atol(argv[4]));
     }
+#if GPU_ACCELERATION
+    if (cmd == "gpu" && argc > 6) {
+        // Simulation::gpu_compute_radiation_field (simulation.cu:512-726)
+        // as its Python binding calls it, reps times; each call builds its
+        // solvers, traces and solves every ray pair and fills J and the ALO
+        // again.  The first call also sets max_npoints_on_rays; the CUDA
+        // context is created before it.
+        set_up(sim, true);
+        const size_t block = (size_t)std::atol(argv[4]), nblocks = (size_t)std::atol(argv[5]);
+        const int reps = std::atoi(argv[6]);
+        if (cudaFree(nullptr) != cudaSuccess) {
+            std::fprintf(stderr, "no CUDA device\n");
+            return 1;
+        }
+        for (int k = 0; k < reps; k++) {
+            const auto t0 = std::chrono::steady_clock::now();
+            const int rc = sim.gpu_compute_radiation_field(1, block, nblocks, 1.0);
+            cudaDeviceSynchronize();
+            const double s =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            const cudaError_t e = cudaGetLastError();
+            std::printf("{\"rep\": %d, \"seconds\": %.6f, \"rc\": %d, \"cuda\": \"%s\", "
+                        "\"threads\": %d, \"max_npoints_on_rays\": %ld}\n",
+                        k, s, rc, cudaGetErrorString(e), omp_get_max_threads(),
+                        (long)sim.geometry.max_npoints_on_rays);
+            std::fflush(stdout);
+            if (rc != 0 || e != cudaSuccess) return 1;
+        }
+        sim.compute_Jeff();
+        std::vector<double> J(sim.radiation.J.size());
+        for (size_t i = 0; i < J.size(); i++) J[i] = sim.radiation.J[i];
+        write_raw(out + "/J.bin", J);
+        write_line_fields(sim, out);
+        return 0;
+    }
+#endif
     std::fprintf(stderr, "unknown command %s\n", cmd.c_str());
     return 2;
 }

@@ -1,7 +1,9 @@
-// configure.hpp for compiling the reference's CPU path as a test oracle:
-// one process, OpenMP threads, no MPI, no Grid-SIMD, no GPU, no Python IO.
-// It shadows the reference's checked-in src/configure.hpp (which enables MPI
-// and the GPU) through the include path.
+// configure.hpp for compiling the reference's code as a test oracle: one
+// process, OpenMP threads, no MPI, no Grid-SIMD, no Python IO.  The GPU
+// path (src/Simulation/Solver/gpu, Simulation::gpu_compute_radiation_field)
+// is compiled in only when MGR_REF_GPU is defined, for the build of the
+// reference's own GPU solver.  It shadows the reference's checked-in
+// src/configure.hpp (which enables MPI and the GPU) through the include path.
 #pragma once
 #define MAGRITTE_FOLDER "."
 #define MAGRITTE_VERSION_MAJOR "0"
@@ -10,4 +12,8 @@
 #define MPI_PARALLEL false
 #define OMP_PARALLEL true
 #define GRID_SIMD false
+#ifdef MGR_REF_GPU
+#define GPU_ACCELERATION true
+#else
 #define GPU_ACCELERATION false
+#endif
