@@ -52,6 +52,11 @@ TOL = 1.0e-4
 MAX_ITER = 400
 FALLBACK_HBM_GBS = 6650.0
 STAGED_DRAM_BYTES_PER_UPDATE = 0.556
+# thread instructions (warp instructions x 32) per update of the same kernel
+# in the same capture: the issue-bound ceiling is 148 SMs x 4 schedulers x
+# the SM clock x 32 lanes / this
+STAGED_THREAD_INST_PER_UPDATE = 42.6
+B200_SMS = 148
 
 
 def parse():
@@ -95,6 +100,8 @@ WORKLOADS = {
     "wind64": ("64^3 spherical wind, 10-level rotor", "config2", "wind_rotor10.npz"),
     "wind32": ("32^3 spherical wind, 10-level rotor", "wind32", "wind_rotor10.npz"),
     "lattice16": ("16^3 lattice cloud, 2-level line", "config1", None),
+    "lattice16_dense": ("16^3 lattice cloud at 1e3 x density (line-centre tau ~1e4), "
+                        "2-level line", "config3", None),
     "batch256": ("256 independent spherical winds of 2k-60k points, 20-level rotor, 24 rays",
                  "config4", None),
     "turb128": ("128^3 turbulent cloud, 21-level rotor, 96 rays, 41 bins/line", "config5",
@@ -676,6 +683,17 @@ def run_b200(args):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if traffic is not None:
+        # the bound that holds: instruction issue at the measured clock
+        mhz = (line["clocks"] or {}).get("sm_mhz") or 1965.0
+        ceiling = B200_SMS * 4 * mhz * 1e6 * 32 / STAGED_THREAD_INST_PER_UPDATE
+        ups = solve_upd[-1] / (avg_ms / 1e3)
+        line["roofline"]["issue"] = {
+            "thread_instructions_per_update": STAGED_THREAD_INST_PER_UPDATE,
+            "ceiling_updates_per_s": ceiling, "achieved_updates_per_s": ups,
+            "frac": ups / ceiling,
+            "note": "instructions per update from ncu on the 32^3 wind (same kernel); ceiling = "
+                    "148 SMs x 4 schedulers x SM clock x 32 lanes / instructions per update"}
     if not args.no_cpu_baseline and world == 1:
         from oracle.measure_iterations import step_kinds
         k = step_kinds(iters[-1])
