@@ -256,6 +256,34 @@ mgr_status mgr_get_patch_stats(mgr_handle *h, int64_t *patched, int64_t *fallbac
  * double.  No reference counterpart. */
 mgr_status mgr_set_patch_capacity(mgr_handle *h, int64_t entries);
 
+/* parameters.n_off_diag (Model/parameters.hpp:87): 0 or 1 keep the
+ * diagonal ALO (the reference's n_off_diag = 1 adds no off-diagonal
+ * element, raypair_lambda.tpp:129); M = 2 .. 8 keep, for every cell, line
+ * and ray pair, the M-1 nearest off-diagonal elements of the origin's row on
+ * each side (RayPair::solve's non-local branch, raypair_solver.tpp:336-388,
+ * with RayPair::update_Lambda's weights, raypair_lambda.tpp:94-149), use
+ * them in compute_Jeff (sim_lines.tpp:176-220), and solve the rate
+ * equations of all cells as one system (lineProducingSpecies.tpp:249-495,
+ * SparseLU there, block-Jacobi sweeps here).  Where the reference reads
+ * other elements (L_lower[m][n_ar-m] is the element (n_ar+1, n_ar-m)) and
+ * places the upper-level term of an element at (I(nr), I(nr)) instead of
+ * (I(p), I(nr)), this follows the origin's row and the placement whose
+ * terms cancel at convergence, so the iteration keeps the local-ALO fixed
+ * point.  One whole model only (MGR_ERR_UNSUPPORTED with a batch or an
+ * origin range); each formal solve adds one FP64 kernel, and the ALI
+ * iteration is not graph-captured. */
+mgr_status mgr_set_n_off_diag(mgr_handle *h, int32_t n_off_diag);
+
+/* The non-local ALO elements of the last formal solve (n_off_diag = M >= 2):
+ * Loff [ncells][nrad][nrays/2][2][M-1] (side 0: the front trace, the longer
+ * one of the pair, side 1 the back trace; distance 1 .. M-1 from the
+ * origin) and their cells Loff_nr [ncells][nrays/2][2][M-1] (-1: no point
+ * there).  Either pointer may be NULL. */
+mgr_status mgr_get_alo_nonlocal(mgr_handle *h, double *Loff, int64_t *Loff_nr);
+
+/* Block-Jacobi sweeps of the last non-local statistical-equilibrium solve. */
+mgr_status mgr_get_nonlocal_sweeps(mgr_handle *h, int64_t *sweeps);
+
 /* Synchronises the handle's stream. */
 mgr_status mgr_synchronize(mgr_handle *h);
 

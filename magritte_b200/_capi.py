@@ -42,7 +42,8 @@ EXPORTS = (
     "mgr_get_device_buffer", "mgr_get_population_history", "mgr_set_population_history",
     "mgr_compute_image", "mgr_set_patch_capacity", "mgr_set_scattering_terms",
     "mgr_get_scattering_terms", "mgr_compute_radiation_field_scattering", "mgr_get_scattering_uv",
-    "mgr_calc_U_and_V", "mgr_get_solve_breakdown",
+    "mgr_calc_U_and_V", "mgr_get_solve_breakdown", "mgr_set_n_off_diag", "mgr_get_alo_nonlocal",
+    "mgr_get_nonlocal_sweeps",
 )
 # mgr_buffer
 BUF_POPULATION, BUF_PREV1, BUF_PREV2, BUF_PREV3, BUF_JLIN, BUF_LAMBDA, BUF_PARTIALS = range(7)
@@ -152,6 +153,9 @@ def load(build_if_missing: bool = True):
     L.mgr_get_population_history.argtypes = [_P, _P, _P, _P]
     L.mgr_compute_image.argtypes = [_P, _i64, _dbl, _P, _P, _P, _P, _P]
     L.mgr_set_patch_capacity.argtypes = [_P, _i64]
+    L.mgr_set_n_off_diag.argtypes = [_P, C.c_int32]
+    L.mgr_get_alo_nonlocal.argtypes = [_P, _P, _P]
+    L.mgr_get_nonlocal_sweeps.argtypes = [_P, _P]
     L.mgr_set_scattering_terms.argtypes = [_P, _P, _P]
     L.mgr_get_scattering_terms.argtypes = [_P, _P, _P]
     L.mgr_compute_radiation_field_scattering.argtypes = [_P]

@@ -116,6 +116,16 @@ struct mgr_handle {
     // scattering: terms U, V and the origins' u, v per (pair, cell, bin)
     double *scat_U = nullptr, *scat_V = nullptr, *scat_u = nullptr, *scat_v = nullptr;
 
+    // non-local ALO (parameters.n_off_diag >= 2): the off-diagonal elements
+    // and their cells, the block-Jacobi iterates and the sweep's max change
+    int noff = 0;
+    double *Loff = nullptr;
+    int32_t *Loff_nr = nullptr;
+    double *nl_x[2] = {nullptr, nullptr};
+    double *nl_change = nullptr;
+    double *h_nl_change = nullptr;     // pinned
+    int64_t nl_sweeps = 0;             // block-Jacobi sweeps of the last solve
+
     // warm start: features, LTE log fractions, network output and the
     // network's parameters, kept between calls (allocated once per model)
     float *ws_F = nullptr, *ws_L = nullptr, *ws_D = nullptr, *ws_P = nullptr;
@@ -233,8 +243,11 @@ void free_model(mgr_handle *h) {
     h->model_allocs.clear();
     void **ws[] = {(void **)&h->ws_F, (void **)&h->ws_L, (void **)&h->ws_D, (void **)&h->ws_P,
                    (void **)&h->ws_mean, (void **)&h->ws_istd, (void **)&h->scat_U,
-                   (void **)&h->scat_V, (void **)&h->scat_u, (void **)&h->scat_v};
+                   (void **)&h->scat_V, (void **)&h->scat_u, (void **)&h->scat_v,
+                   (void **)&h->Loff, (void **)&h->Loff_nr, (void **)&h->nl_x[0],
+                   (void **)&h->nl_x[1], (void **)&h->nl_change};
     for (void **p : ws) free_ptr(*p);
+    h->noff = 0;
     h->ws_np = 0;
     void **state[] = {(void **)&h->pop, (void **)&h->prev1, (void **)&h->prev2, (void **)&h->prev3,
                       (void **)&h->eps, (void **)&h->kap, (void **)&h->Jlin, (void **)&h->Lam,
@@ -484,6 +497,10 @@ void do_upload(mgr_handle *h, const mgr_model_desc *d) {
     m.win_lo = upload(h, wlo.data(), d->nrad, T);
     m.win_hi = upload(h, whi.data(), d->nrad, T);
     m.roots = upload(h, d->quad_roots, d->nquads, T);
+    {
+        const double span = d->quad_roots[d->nquads - 1] - d->quad_roots[0];
+        m.root_inv_step = (d->nquads > 1 && span > 0.0) ? (double)(d->nquads - 1) / span : 0.0;
+    }
     m.qw = upload(h, d->quad_weights, d->nquads, T);
     m.pop_tot = upload(h, d->population_tot, N, T);
     for (int c = 0; c < d->ncolpar; c++) {
@@ -867,6 +884,14 @@ void enqueue_redo(mgr_handle *h, const TraceView &t, int64_t done, int64_t count
     h->fp64_fallbacks += count - done;
 }
 
+// The non-local ALO elements of origins [s_begin, s_end) of a trace store
+// (FP64, whatever the precision of the solve).
+void enqueue_offdiag(mgr_handle *h, const TraceView &t, int64_t s_begin, int64_t s_end) {
+    OffdiagArgs oa{h->eps, h->kap, h->Loff, h->Loff_nr, h->noff - 1, s_begin, s_end};
+    ck(launch_offdiag(h->mv, t, oa, h->flags, h->stream), "off-diagonal ALO");
+    h->launches += 1;
+}
+
 void finish_solve(mgr_handle *h, int precision, int variant, bool timing, int64_t patched) {
     if (precision == MGR_MIXED && h->stored && h->h_flags->redo_count > 0) {
         // more float failures than the patch list holds: the listed origins
@@ -916,6 +941,12 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
         finish_solve(h, precision, variant, timing,
                      precision == MGR_MIXED ? (int64_t)*h->h_patch : 0);
         h->last_trace_ms = 0.0;
+        if (h->noff >= 2) {
+            TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
+            enqueue_offdiag(h, t, h->o_begin, h->o_end);
+            ck(cudaStreamSynchronize(h->stream), "off-diagonal ALO");
+            check_flags(h, "off-diagonal ALO");
+        }
         return;
     }
     // traces in batches of origins, rebuilt for every solve
@@ -946,6 +977,7 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
            "formal solve");
         h->tune[precision == MGR_MIXED].kind = kind;
         h->launches += precision == MGR_MIXED ? 2 : 1;
+        if (h->noff >= 2) enqueue_offdiag(h, t, 0, cnt);
         if (precision == MGR_MIXED) {
             ck(cudaMemcpyAsync(h->h_patch, h->patch_count, sizeof(unsigned long long),
                                cudaMemcpyDeviceToHost, h->stream), "d2h");
@@ -998,8 +1030,69 @@ int enqueue_stats(mgr_handle *h, const LevelArgs &a) {
     return n;
 }
 
+NonlocalArgs nonlocal_args(mgr_handle *h) {
+    return NonlocalArgs{h->Loff, h->Loff_nr, h->noff - 1, h->nl_x[0], h->nl_x[1], h->nl_change};
+}
+
+// Statistical equilibrium with the non-local ALO: the rate equations of all
+// cells as one system, solved by block-Jacobi sweeps from the populations
+// before the solve until no population changes by more than 1e-14 of
+// itself (of 1e-10 of its cell's total below that), or, once below 1e-8,
+// the change sets no new low for three sweeps (the rounding floor of the
+// cell solves); then the statistics and emissivities/opacities.  The host
+// reads each sweep's change, so this step is not graph-captured.
+int stateq_nonlocal(mgr_handle *h) {
+    const LevelArgs a = level_args(h);
+    reset_flags(h);
+    const int64_t NL = h->N * h->nlev;
+    ck(launch_history_shift(h->mv, a, h->stream), "history");
+    ck(cudaMemcpyAsync(h->nl_x[0], h->prev1, NL * sizeof(double), cudaMemcpyDeviceToDevice,
+                       h->stream), "iterate");
+    NonlocalArgs nl = nonlocal_args(h);
+    const int nb = nonlocal_sweep_blocks(h->mv);
+    int cur = 0, launches = 2, best_sweep = 0;
+    double best = INFINITY;
+    bool ok = false;
+    int64_t sweep = 0;
+    for (; sweep < 1000; sweep++) {
+        nl.x_in = h->nl_x[cur];
+        nl.x_out = h->nl_x[1 - cur];
+        ck(launch_stateq_nonlocal_sweep(h->mv, a, nl, h->flags, h->stream), "stateq sweep");
+        ck(cudaMemcpyAsync(h->h_nl_change, h->nl_change + nb, sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream), "change");
+        ck(cudaStreamSynchronize(h->stream), "stateq sweep");
+        launches += 2;
+        cur = 1 - cur;
+        const double change = *h->h_nl_change;
+        if (!(change == change)) break;   // NaN: a singular block (lu_err is set)
+        if (change <= 1.0E-14) { ok = true; break; }
+        if (change < best) {
+            best = change;
+            best_sweep = (int)sweep;
+        } else if (best < 1.0E-8 && sweep >= best_sweep + 3) {
+            ok = true;
+            break;
+        }
+    }
+    h->nl_sweeps = sweep + 1;
+    ck(cudaMemcpyAsync(h->pop, h->nl_x[cur], NL * sizeof(double), cudaMemcpyDeviceToDevice,
+                       h->stream), "populations");
+    ck(launch_convergence(h->mv, a, h->stream), "convergence");
+    ck(launch_emissivity_opacity(h->mv, a, h->stream), "emissivity");
+    launches += 3;
+    const int n = enqueue_stats(h, a);
+    if (!ok) {
+        ck(cudaStreamSynchronize(h->stream), "stats");
+        if (h->h_flags->lu_err == 0)
+            fail(MGR_ERR_LU_SINGULAR,
+                 "non-local rate equations: block Jacobi did not converge in 1000 sweeps");
+    }
+    return launches + n;
+}
+
 // Statistical equilibrium (+ statistics); returns the kernels launched.
 int enqueue_stateq(mgr_handle *h) {
+    if (h->noff >= 2) return stateq_nonlocal(h);
     const LevelArgs a = level_args(h);
     reset_flags(h);
     ck(launch_stateq(h->mv, a, h->flags, h->stream), "stateq");
@@ -1008,7 +1101,8 @@ int enqueue_stateq(mgr_handle *h) {
 
 // Jeff, statistical equilibrium and statistics after a formal solve.
 int enqueue_level(mgr_handle *h) {
-    ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
+    if (h->noff >= 2) ck(launch_jeff_nonlocal(h->mv, level_args(h), nonlocal_args(h), h->stream), "jeff");
+    else ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
     return 1 + enqueue_stateq(h);
 }
 
@@ -1106,6 +1200,7 @@ mgr_status mgr_destroy(mgr_handle *h) {
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->h_patch) cudaFreeHost(h->h_patch);
     if (h->h_tstats) cudaFreeHost(h->h_tstats);
+    if (h->h_nl_change) cudaFreeHost(h->h_nl_change);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->tev0) cudaEventDestroy(h->tev0);
@@ -1237,7 +1332,10 @@ mgr_status mgr_compute_radiation_field(mgr_handle *h, int32_t precision) {
 mgr_status mgr_compute_Jeff(mgr_handle *h) {
     return run(h, [&] {
         need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
-        ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
+        if (h->noff >= 2)
+            ck(launch_jeff_nonlocal(h->mv, level_args(h), nonlocal_args(h), h->stream), "jeff");
+        else
+            ck(launch_jeff(h->mv, level_args(h), h->stream), "jeff");
         h->launches += 1;
         ck(cudaStreamSynchronize(h->stream), "jeff sync");
     });
@@ -1255,6 +1353,7 @@ mgr_status mgr_set_origin_range(mgr_handle *h, int64_t o_begin, int64_t o_end) {
     return run(h, [&] {
         need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
         need(h->nseg == 0, MGR_ERR_UNSUPPORTED, "a batch of models is not partitioned");
+        need(h->noff < 2, MGR_ERR_UNSUPPORTED, "a non-local ALO run is not partitioned");
         need(0 <= o_begin && o_begin < o_end && o_end <= h->N, MGR_ERR_INVALID_ARG,
              "origin range outside [0, ncells)");
         need(o_begin % kCellsPerPartial == 0 && (o_end % kCellsPerPartial == 0 || o_end == h->N),
@@ -1334,7 +1433,7 @@ mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts
         need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
         need(h->whole(), MGR_ERR_STATE,
              "a shard (origin range) iterates through a partitioned driver, not this loop");
-        const bool graph = opts->use_graph != 0;
+        const bool graph = opts->use_graph != 0 && h->noff < 2;   // non-local: host-driven sweeps
         auto converged = [&](double fnc, double mx) {
             return opts->tol_max_rel > 0.0 ? mx < opts->tol_max_rel : !(fnc > 0.005);
         };
@@ -1409,6 +1508,8 @@ mgr_status mgr_set_segments(mgr_handle *h, int64_t nseg, const int64_t *seg_begi
         need(nseg >= 1 && seg_begin != nullptr, MGR_ERR_INVALID_ARG, "need nseg >= 1 and bounds");
         need(seg_begin[0] == 0 && seg_begin[nseg] == h->N, MGR_ERR_INVALID_ARG,
              "model bounds must start at 0 and end at ncells");
+        need(h->noff < 2 || nseg == 1, MGR_ERR_UNSUPPORTED,
+             "a batch of models runs with the local ALO (n_off_diag 0 or 1)");
         for (int64_t g = 0; g < nseg; g++)
             need(seg_begin[g + 1] > seg_begin[g], MGR_ERR_INVALID_ARG, "empty or unordered model");
         set_device(h);
@@ -1580,6 +1681,61 @@ mgr_status mgr_set_patch_capacity(mgr_handle *h, int64_t entries) {
         free_ptr((void *&)h->redo_list);
         h->patch_cap_set = entries;
         h->gen++;
+    });
+}
+
+mgr_status mgr_set_n_off_diag(mgr_handle *h, int32_t n_off_diag) {
+    return run(h, [&] {
+        need(h->model_loaded, MGR_ERR_STATE, "no model uploaded");
+        need(n_off_diag >= 0 && n_off_diag <= kMaxOffDiag, MGR_ERR_INVALID_ARG,
+             "n_off_diag outside 0 .. 8");
+        need(n_off_diag < 2 || (h->whole() && h->nseg == 0), MGR_ERR_UNSUPPORTED,
+             "the non-local ALO runs on one whole model (no batch, no origin range)");
+        need(h->nlev <= kMaxLevels, MGR_ERR_UNSUPPORTED, "too many levels");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        void **bufs[] = {(void **)&h->Loff, (void **)&h->Loff_nr, (void **)&h->nl_x[0],
+                         (void **)&h->nl_x[1], (void **)&h->nl_change};
+        for (void **b : bufs) free_ptr(*b);
+        h->noff = n_off_diag;
+        if (n_off_diag >= 2) {
+            const int64_t ne = (int64_t)h->npairs * 2 * (n_off_diag - 1);
+            h->Loff = dalloc<double>(h, h->N * h->nrad * ne, nullptr);
+            h->Loff_nr = dalloc<int32_t>(h, h->N * ne, nullptr);
+            ck(cudaMemsetAsync(h->Loff, 0, h->N * h->nrad * ne * sizeof(double), h->stream), "zero");
+            ck(cudaMemsetAsync(h->Loff_nr, 0xff, h->N * ne * sizeof(int32_t), h->stream), "zero");
+            h->nl_x[0] = dalloc<double>(h, h->N * h->nlev, nullptr);
+            h->nl_x[1] = dalloc<double>(h, h->N * h->nlev, nullptr);
+            h->nl_change = dalloc<double>(h, nonlocal_sweep_blocks(h->mv) + 1, nullptr);
+            if (!h->h_nl_change) ck(cudaMallocHost(&h->h_nl_change, sizeof(double)), "pinned");
+            ck(cudaStreamSynchronize(h->stream), "sync");
+        }
+        h->gen++;
+    });
+}
+
+mgr_status mgr_get_alo_nonlocal(mgr_handle *h, double *Loff, int64_t *Loff_nr) {
+    return run(h, [&] {
+        need(h->noff >= 2, MGR_ERR_STATE, "n_off_diag < 2: the ALO is diagonal");
+        set_device(h);
+        ck(cudaStreamSynchronize(h->stream), "sync");
+        const int64_t ne = (int64_t)h->npairs * 2 * (h->noff - 1);
+        if (Loff)
+            ck(cudaMemcpy(Loff, h->Loff, h->N * h->nrad * ne * sizeof(double),
+                          cudaMemcpyDeviceToHost), "d2h");
+        if (Loff_nr) {
+            std::vector<int32_t> tmp(h->N * ne);
+            ck(cudaMemcpy(tmp.data(), h->Loff_nr, tmp.size() * sizeof(int32_t),
+                          cudaMemcpyDeviceToHost), "d2h");
+            for (size_t i = 0; i < tmp.size(); i++) Loff_nr[i] = tmp[i];
+        }
+    });
+}
+
+mgr_status mgr_get_nonlocal_sweeps(mgr_handle *h, int64_t *sweeps) {
+    return run(h, [&] {
+        need(sweeps != nullptr, MGR_ERR_INVALID_ARG, "NULL output");
+        *sweeps = h->nl_sweeps;
     });
 }
 

@@ -104,6 +104,119 @@ __device__ __forceinline__ void block_reduce3(double &cnt, double &sum, double &
     }
 }
 
+// Rows of cell p's block of RT (transpose convention,
+// lineProducingSpecies.tpp:282-389) owned by lane i: radiative rates, the
+// local ALO element (nr = p) with the opacity of the populations `old`,
+// collisions, and the conservation row replacing the last level's.
+__device__ __forceinline__ void assemble_rows(const ModelView &m, const LevelArgs &a, int64_t p,
+                                              int i, double *row, double *y, const double *old) {
+    const int nl = m.nlev, K = m.nrad, last = nl - 1;
+    // radiative transitions
+    for (int k = 0; k < K; k++) {
+        const int I = m.irad[k], J = m.jrad[k];
+        if (i != I && i != J) continue;
+        const double Jeff = a.Jeff[p * K + k];
+        const double v_IJ = m.A[k] + m.Bs[k] * Jeff;
+        const double v_JI = m.Ba[k] * Jeff;
+        if (J != last && i == J) { row[I] += v_IJ; row[J] += -v_JI; }
+        if (I != last && i == I) { row[J] += v_JI; row[I] += -v_IJ; }
+    }
+    // approximated Lambda operator (nr = p)
+    for (int k = 0; k < K; k++) {
+        const int I = m.irad[k], J = m.jrad[k];
+        if (i != I && i != J) continue;
+        const double opac = kHH_OVER_FOUR_PI * (old[J] * m.Ba[k] - old[I] * m.Bs[k]);
+        const double v_IJ = -a.Lam[p * K + k] * opac;
+        if (J != last && i == J) row[I] += v_IJ;
+        if (I != last && i == I) row[I] += -v_IJ;
+    }
+    // collisions
+    for (int c = 0; c < m.ncolpar; c++) {
+        const ColparDev &cp = m.colpar[c];
+        double abn = cp.abn[p];
+        const double tmp = m.T[p];
+        if (cp.ortho_para != 0) {
+            const double frac_H2_para = 1.0 / (1.0 + 9.0 * exp(-170.5 / tmp));
+            if (cp.ortho_para == 1) abn *= (1.0 - frac_H2_para);
+            if (cp.ortho_para == 2) abn *= frac_H2_para;
+        }
+        int t;
+        double step;
+        colpar_position(cp, tmp, t, step);
+        for (int k = 0; k < cp.ncol; k++) {
+            const int I = cp.icol[k], J = cp.jcol[k];
+            if (i != I && i != J) continue;
+            double Cd, Ce;
+            if (t == 0) {
+                Cd = cp.Cd[k];
+                Ce = cp.Ce[k];
+            } else {
+                const double cd0 = cp.Cd[(t - 1) * cp.ncol + k], cd1 = cp.Cd[t * cp.ncol + k];
+                const double ce0 = cp.Ce[(t - 1) * cp.ncol + k], ce1 = cp.Ce[t * cp.ncol + k];
+                Cd = cd0 + (cd1 - cd0) * step;
+                Ce = ce0 + (ce1 - ce0) * step;
+            }
+            const double v_IJ = Cd * abn, v_JI = Ce * abn;
+            if (J != last && i == J) { row[I] += v_IJ; row[J] += -v_JI; }
+            if (I != last && i == I) { row[J] += v_JI; row[I] += -v_IJ; }
+        }
+    }
+    if (i == last) {
+        for (int j = 0; j < nl; j++) row[j] += 1.0;
+        y[last] = m.pop_tot[p];
+    }
+}
+
+// Partial-pivot LU of the nl x nl rows M (pitch kRowPitch) with right-hand
+// side y, one lane per row; returns true on a zero pivot.  The pivot search
+// is a butterfly over the lanes, its result taken from lane 0.
+__device__ __forceinline__ bool warp_lu(double *M, double *y, int nl, int i) {
+    bool singular = false;
+    for (int kc = 0; kc < nl; kc++) {
+        double v = (i >= kc && i < nl) ? fabs(M[i * kRowPitch + kc]) : -1.0;
+        int idx = i;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, v, s);
+            const int oi = __shfl_xor_sync(0xffffffffu, idx, s);
+            if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+        }
+        // lane 0's result for everyone: NaNs can make the butterfly
+        // disagree between lanes, and the loop must stay warp-uniform
+        v = __shfl_sync(0xffffffffu, v, 0);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (!(v > 0.0) || idx >= nl) { singular = true; break; }
+        if (idx != kc) {
+            if (i < nl) {
+                const double t0 = M[kc * kRowPitch + i];
+                M[kc * kRowPitch + i] = M[idx * kRowPitch + i];
+                M[idx * kRowPitch + i] = t0;
+            }
+            if (i == 0) { const double t1 = y[kc]; y[kc] = y[idx]; y[idx] = t1; }
+        }
+        __syncwarp();
+        if (i > kc && i < nl) {
+            const double l = M[i * kRowPitch + kc] * (1.0 / M[kc * kRowPitch + kc]);
+            if (l != 0.0) {
+                for (int j = kc + 1; j < nl; j++) M[i * kRowPitch + j] -= l * M[kc * kRowPitch + j];
+                y[i] -= l * y[kc];
+            }
+        }
+        __syncwarp();
+    }
+    return singular;
+}
+
+// Back substitution after warp_lu: y becomes the solution.
+__device__ __forceinline__ void warp_back_substitute(const double *M, double *y, int nl, int i) {
+    for (int jc = nl - 1; jc >= 0; jc--) {
+        if (i == jc) y[jc] = y[jc] / M[jc * kRowPitch + jc];
+        __syncwarp();
+        if (i < jc) y[i] -= M[i * kRowPitch + jc] * y[jc];
+        __syncwarp();
+    }
+}
+
 // One warp per cell: assemble the cell's block of RT (transpose convention,
 // lineProducingSpecies.tpp:282-389), solve it, update populations and their
 // history, then convergence partials and the cell's emissivities/opacities.
@@ -117,7 +230,7 @@ __global__ void __launch_bounds__(kStateqWarps * 32) stateq_kernel(ModelView m, 
     const int64_t p = a.c_begin + (int64_t)blockIdx.x * kStateqWarps + warp;
     // cells of a converged model of a batch keep their populations
     const bool valid = p < a.c_end && !(m.seg_active && !m.seg_active[m.cell_seg[p]]);
-    const int nl = m.nlev, K = m.nrad, last = nl - 1;
+    const int nl = m.nlev, K = m.nrad;
     double *M = Msh[warp];
     double *y = ysh[warp];
     double *old = popsh[warp];
@@ -135,107 +248,13 @@ __global__ void __launch_bounds__(kStateqWarps * 32) stateq_kernel(ModelView m, 
             y[i] = 0.0;
         }
         __syncwarp();
-        if (i < nl) {
-            double *row = M + i * kRowPitch;
-            // radiative transitions
-            for (int k = 0; k < K; k++) {
-                const int I = m.irad[k], J = m.jrad[k];
-                if (i != I && i != J) continue;
-                const double Jeff = a.Jeff[p * K + k];
-                const double v_IJ = m.A[k] + m.Bs[k] * Jeff;
-                const double v_JI = m.Ba[k] * Jeff;
-                if (J != last && i == J) { row[I] += v_IJ; row[J] += -v_JI; }
-                if (I != last && i == I) { row[J] += v_JI; row[I] += -v_IJ; }
-            }
-            // approximated Lambda operator (nr = p)
-            for (int k = 0; k < K; k++) {
-                const int I = m.irad[k], J = m.jrad[k];
-                if (i != I && i != J) continue;
-                const double opac = kHH_OVER_FOUR_PI * (old[J] * m.Ba[k] - old[I] * m.Bs[k]);
-                const double v_IJ = -a.Lam[p * K + k] * opac;
-                if (J != last && i == J) row[I] += v_IJ;
-                if (I != last && i == I) row[I] += -v_IJ;
-            }
-            // collisions
-            for (int c = 0; c < m.ncolpar; c++) {
-                const ColparDev &cp = m.colpar[c];
-                double abn = cp.abn[p];
-                const double tmp = m.T[p];
-                if (cp.ortho_para != 0) {
-                    const double frac_H2_para = 1.0 / (1.0 + 9.0 * exp(-170.5 / tmp));
-                    if (cp.ortho_para == 1) abn *= (1.0 - frac_H2_para);
-                    if (cp.ortho_para == 2) abn *= frac_H2_para;
-                }
-                int t;
-                double step;
-                colpar_position(cp, tmp, t, step);
-                for (int k = 0; k < cp.ncol; k++) {
-                    const int I = cp.icol[k], J = cp.jcol[k];
-                    if (i != I && i != J) continue;
-                    double Cd, Ce;
-                    if (t == 0) {
-                        Cd = cp.Cd[k];
-                        Ce = cp.Ce[k];
-                    } else {
-                        const double cd0 = cp.Cd[(t - 1) * cp.ncol + k], cd1 = cp.Cd[t * cp.ncol + k];
-                        const double ce0 = cp.Ce[(t - 1) * cp.ncol + k], ce1 = cp.Ce[t * cp.ncol + k];
-                        Cd = cd0 + (cd1 - cd0) * step;
-                        Ce = ce0 + (ce1 - ce0) * step;
-                    }
-                    const double v_IJ = Cd * abn, v_JI = Ce * abn;
-                    if (J != last && i == J) { row[I] += v_IJ; row[J] += -v_JI; }
-                    if (I != last && i == I) { row[J] += v_JI; row[I] += -v_IJ; }
-                }
-            }
-            if (i == last) {
-                for (int j = 0; j < nl; j++) row[j] += 1.0;
-                y[last] = m.pop_tot[p];
-            }
-        }
+        if (i < nl) assemble_rows(m, a, p, i, M + i * kRowPitch, y, old);
         __syncwarp();
-        // partial-pivot LU, lane = row
-        bool singular = false;
-        for (int kc = 0; kc < nl; kc++) {
-            double v = (i >= kc && i < nl) ? fabs(M[i * kRowPitch + kc]) : -1.0;
-            int idx = i;
-#pragma unroll
-            for (int s = 16; s > 0; s >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, v, s);
-                const int oi = __shfl_xor_sync(0xffffffffu, idx, s);
-                if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
-            }
-            // lane 0's result for everyone: NaNs can make the butterfly
-            // disagree between lanes, and the loop must stay warp-uniform
-            v = __shfl_sync(0xffffffffu, v, 0);
-            idx = __shfl_sync(0xffffffffu, idx, 0);
-            if (!(v > 0.0) || idx >= nl) { singular = true; break; }
-            if (idx != kc) {
-                if (i < nl) {
-                    const double t0 = M[kc * kRowPitch + i];
-                    M[kc * kRowPitch + i] = M[idx * kRowPitch + i];
-                    M[idx * kRowPitch + i] = t0;
-                }
-                if (i == 0) { const double t1 = y[kc]; y[kc] = y[idx]; y[idx] = t1; }
-            }
-            __syncwarp();
-            if (i > kc && i < nl) {
-                const double l = M[i * kRowPitch + kc] * (1.0 / M[kc * kRowPitch + kc]);
-                if (l != 0.0) {
-                    for (int j = kc + 1; j < nl; j++) M[i * kRowPitch + j] -= l * M[kc * kRowPitch + j];
-                    y[i] -= l * y[kc];
-                }
-            }
-            __syncwarp();
-        }
+        const bool singular = warp_lu(M, y, nl, i);
         if (singular) {
             if (lane == 0) atomicAdd(&flags->lu_err, 1ull);
         } else {
-            for (int jc = nl - 1; jc >= 0; jc--) {
-                if (i == jc) y[jc] = y[jc] / M[jc * kRowPitch + jc];
-                __syncwarp();
-                if (i < jc) y[i] -= M[i * kRowPitch + jc] * y[jc];
-                __syncwarp();
-            }
+            warp_back_substitute(M, y, nl, i);
             if (i < nl) {
                 const double nw = y[i];
                 a.pop[p * nl + i] = nw;
@@ -264,6 +283,125 @@ __global__ void __launch_bounds__(kStateqWarps * 32) stateq_kernel(ModelView m, 
         a.partials[3 * g + 0] = cnt;
         a.partials[3 * g + 1] = rsum;
         a.partials[3 * g + 2] = rmax;
+    }
+}
+
+// ------------------------------------------------------------ non-local ALO
+//
+// With n_off_diag = M >= 2 every (cell p, line k) also holds the M-1 nearest
+// off-diagonal ALO elements on each side of every ray pair (NonlocalArgs),
+// each belonging to the cell nr the ray passes there.
+
+// compute_Jeff (sim_lines.tpp:176-220) over every element of (p, k): the
+// diagonal one, then the non-local ones in (pair, side, distance) order.
+__global__ void jeff_nonlocal_kernel(ModelView m, LevelArgs a, NonlocalArgs nl) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= m.N * m.nrad) return;
+    const int64_t p = idx / m.nrad;
+    const int k = (int)(idx - p * m.nrad);
+    const int I = m.irad[k], nlev = m.nlev;
+    const int64_t ne = (int64_t)m.npairs * 2 * nl.M1;
+    double diff = a.Lam[idx] * a.pop[p * nlev + I];
+    for (int64_t e = 0; e < ne; e++) {
+        const int c = nl.Loff_nr[p * ne + e];
+        if (c < 0) continue;
+        diff += nl.Loff[idx * ne + e] * a.pop[(int64_t)c * nlev + I];
+    }
+    a.Jeff[idx] = a.Jlin[idx] - kHH_OVER_FOUR_PI * diff;
+}
+
+// One block-Jacobi sweep of the rate equations of all cells
+// (lineProducingSpecies.tpp:249-495 with n_off_diag > 0): cell p's block as
+// stateq_kernel assembles it from the populations before the solve (prev1,
+// the history already shifted), plus every non-local element (nr, Ls) of
+// the cell with v = -Ls * opacity(p, k): v at (J(p), I(nr)) and -v at
+// (I(p), I(nr)) -- in the block when nr = p, otherwise moved to the
+// right-hand side with nr's populations from x_in.  The solution goes to
+// x_out; change[block] receives the largest change of the block's cells
+// relative to the population (or to 1e-10 of the cell's total below that).
+__global__ void __launch_bounds__(kStateqWarps * 32) stateq_nonlocal_kernel(ModelView m,
+                                                                            LevelArgs a,
+                                                                            NonlocalArgs nl,
+                                                                            DevFlags *flags) {
+    __shared__ double Msh[kStateqWarps][kMaxLevels * kRowPitch];
+    __shared__ double ysh[kStateqWarps][kMaxLevels];
+    __shared__ double popsh[kStateqWarps][kMaxLevels];
+    __shared__ double red[kStateqWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t p = (int64_t)blockIdx.x * kStateqWarps + warp;
+    const int nlev = m.nlev, K = m.nrad, last = nlev - 1;
+    const int64_t ne = (int64_t)m.npairs * 2 * nl.M1;
+    double *M = Msh[warp];
+    double *y = ysh[warp];
+    double *old = popsh[warp];
+    double change = 0.0;
+    if (p < m.N) {
+        const int i = lane;
+        if (i < nlev) {
+            old[i] = a.prev1[p * nlev + i];
+            for (int j = 0; j < nlev; j++) M[i * kRowPitch + j] = 0.0;
+            y[i] = 0.0;
+        }
+        __syncwarp();
+        if (i < nlev) {
+            double *row = M + i * kRowPitch;
+            assemble_rows(m, a, p, i, row, y, old);
+            for (int k = 0; k < K; k++) {
+                const int I = m.irad[k], J = m.jrad[k];
+                if (i != I && i != J) continue;
+                const double opac = kHH_OVER_FOUR_PI * (old[J] * m.Ba[k] - old[I] * m.Bs[k]);
+                for (int64_t e = 0; e < ne; e++) {
+                    const int c = nl.Loff_nr[p * ne + e];
+                    if (c < 0) continue;
+                    const double v = -nl.Loff[(p * K + k) * ne + e] * opac;
+                    if (c == p) {
+                        if (J != last && i == J) row[I] += v;
+                        if (I != last && i == I) row[I] += -v;
+                    } else {
+                        const double xc = nl.x_in[(int64_t)c * nlev + I];
+                        if (J != last && i == J) y[J] -= v * xc;
+                        if (I != last && i == I) y[I] += v * xc;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        const bool singular = warp_lu(M, y, nlev, i);
+        if (singular) {
+            if (lane == 0) atomicAdd(&flags->lu_err, 1ull);
+        } else {
+            warp_back_substitute(M, y, nlev, i);
+            if (i < nlev) {
+                const double v = y[i];
+                const double prev = nl.x_in[p * nlev + i];
+                change = fabs(v - prev) / fmax(fabs(v), 1.0E-10 * m.pop_tot[p]);
+                nl.x_out[p * nlev + i] = v;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) change = fmax(change, __shfl_xor_sync(0xffffffffu, change, s));
+    if (lane == 0) red[warp] = change;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int w = 0; w < kStateqWarps; w++) mx = fmax(mx, red[w]);
+        nl.change[blockIdx.x] = mx;
+    }
+}
+
+// Largest of the per-block changes into change[nblocks] (one block).
+__global__ void max_reduce_kernel(double *change, int nblocks) {
+    __shared__ double red[32];
+    double mx = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) mx = fmax(mx, change[b]);
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, s));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) mx = fmax(mx, red[w]);
+        change[nblocks] = mx;
     }
 }
 
@@ -450,6 +588,31 @@ cudaError_t launch_stateq(const ModelView &m, const LevelArgs &a, DevFlags *flag
         return cudaGetLastError();
     }
     return launch_convergence_final(m, a, s);
+}
+
+cudaError_t launch_jeff_nonlocal(const ModelView &m, const LevelArgs &a, const NonlocalArgs &nl,
+                                 cudaStream_t s) {
+    jeff_nonlocal_kernel<<<blocks_for(m.N * m.nrad, 256), 256, 0, s>>>(m, a, nl);
+    return cudaGetLastError();
+}
+
+int nonlocal_sweep_blocks(const ModelView &m) { return (int)blocks_for(m.N, kStateqWarps); }
+
+cudaError_t launch_history_shift(const ModelView &m, const LevelArgs &a, cudaStream_t s) {
+    LevelArgs b = a;
+    b.c_begin = b.c_end = 0;   // every cell
+    history_shift_kernel<<<blocks_for(m.N * m.nlev, 256), 256, 0, s>>>(m, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stateq_nonlocal_sweep(const ModelView &m, const LevelArgs &a,
+                                         const NonlocalArgs &nl, DevFlags *flags, cudaStream_t s) {
+    const unsigned nb = blocks_for(m.N, kStateqWarps);
+    stateq_nonlocal_kernel<<<nb, kStateqWarps * 32, 0, s>>>(m, a, nl, flags);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    max_reduce_kernel<<<1, 1024, 0, s>>>(nl.change, (int)nb);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_convergence_final(const ModelView &m, const LevelArgs &a, cudaStream_t s) {

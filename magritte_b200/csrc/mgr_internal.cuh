@@ -90,6 +90,7 @@ struct ModelView {
     const double *pop_tot;
     ColparDev colpar[kMaxColpar];
     double pop_prec;
+    double root_inv_step;  // (nquads - 1) / (roots[last] - roots[0]), 0 for one root
     double mixed_scale;    // X: power of two scaling the float opacities
     int overlap;           // some line window holds more than its own line
     // batches of independent models (nullptr / 0 for a single model)
@@ -160,6 +161,8 @@ struct BdyCtx {
     const int32_t *cell2bdy;
     const double *ibdy;            // [nboundary][nfreqs] I_bdy on each boundary cell's grid
     const double *pw, *line, *roots;
+    const double *inv_pw, *inv_line;
+    double root_inv_step;
     int nq, nf;
 };
 
@@ -170,6 +173,9 @@ __device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
     c.pw = m.pw;
     c.line = m.line;
     c.roots = m.roots;
+    c.inv_pw = m.inv_pw;
+    c.inv_line = m.inv_line;
+    c.root_inv_step = m.root_inv_step;
     c.nq = m.nquads;
     c.nf = m.nfreqs;
     return c;
@@ -179,10 +185,14 @@ __device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
 // on the table of Simulation::compute_boundary_intensities.  The reference
 // takes the first bin of cell p's grid with freq <= nu_p(f) by a linear
 // search; the grid ascends (lines do not interleave, which the spectral
-// discretisation checks), so the same bin is found by bisection: first the
-// line whose last bin is >= freq, then the bin within that line.
+// discretisation checks), so the same bin is found in two steps: the line
+// whose last bin is >= freq (first the hint k_hint, the line of the bin the
+// frequency was shifted from, checked against its neighbour; otherwise by
+// bisection), then the bin within that line, from a guess on the root grid
+// walked up or down to the first bin >= freq (two checks when the guess is
+// right, which on an evenly spaced root grid it is but for rounding).
 static __device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p,
-                                                         DevFlags *flags) {
+                                                         DevFlags *flags, int k_hint = -1) {
     const int b = __ldg(c.cell2bdy + p);
     if (b < 0) {
         atomicAdd(&flags->trace_err, 1ull);
@@ -195,20 +205,26 @@ static __device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, 
         return radd(line, rmul(rmul(line, pwp), __ldg(c.roots + z)));
     };
     int lo = 0, hi = K;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (freq <= nu_kz(mid, nq - 1)) hi = mid;
-        else lo = mid + 1;
+    if (k_hint >= 0 && k_hint < K && freq <= nu_kz(k_hint, nq - 1) &&
+        (k_hint == 0 || freq > nu_kz(k_hint - 1, nq - 1))) {
+        lo = k_hint;   // the first line whose last bin is >= freq
+    } else {
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (freq <= nu_kz(mid, nq - 1)) hi = mid;
+            else lo = mid + 1;
+        }
     }
     const double *I = c.ibdy + (int64_t)b * nf;
     if (lo == K) return __ldg(I + nf - 1);   // above the grid
     const int k = lo;
-    int zl = 0, zh = nq - 1;
-    while (zl < zh) {
-        const int mid = (zl + zh) >> 1;
-        if (freq <= nu_kz(k, mid)) zh = mid;
-        else zl = mid + 1;
-    }
+    // guess from freq = line (1 + pw root), then the first z with freq <= nu(k, z)
+    // (freq <= nu(k, nq-1) holds, so the upward walk ends at or before it)
+    const double root = (freq * __ldg(c.inv_line + k) - 1.0) * __ldg(c.inv_pw + p);
+    const double zg = ceil((root - __ldg(c.roots)) * c.root_inv_step);
+    int zl = (int)fmin(fmax(zg, 0.0), (double)(nq - 1));
+    while (zl < nq - 1 && freq > nu_kz(k, zl)) zl++;
+    while (zl > 0 && freq <= nu_kz(k, zl - 1)) zl--;
     const int notch = k * nq + zl;
     if (notch == 0 || notch == nf - 1) return __ldg(I + notch);
     const double nu1 = nu_kz(k, zl);
@@ -322,6 +338,39 @@ cudaError_t launch_jeff(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 // reduces them once every shard's partials are in place.
 cudaError_t launch_stateq(const ModelView &m, const LevelArgs &a, DevFlags *flags, cudaStream_t s);
 cudaError_t launch_convergence_final(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+
+// Non-local ALO (n_off_diag = M1 + 1 >= 2).  Element (o, k, r, side, d) of
+// cell o, line k, ray pair r, side 0 (front trace) or 1 (back trace) at
+// distance d = 1..M1 from the origin: Loff[(((o*K + k)*npairs + r)*2 +
+// side)*M1 + d-1], belonging to cell Loff_nr[((o*npairs + r)*2 + side)*M1 +
+// d-1] (-1: the pair has no point there).
+struct NonlocalArgs {
+    const double *Loff;
+    const int32_t *Loff_nr;
+    int M1;
+    const double *x_in;   // [N*nlev] populations the couplings between cells use
+    double *x_out;        // [N*nlev] solution of the sweep
+    double *change;       // [nonlocal_sweep_blocks + 1]: per block, then the max
+};
+struct OffdiagArgs {
+    const double *eps, *kap;   // [N*K]
+    double *Loff;
+    int32_t *Loff_nr;
+    int M1;
+    int64_t s_begin, s_end;    // origins of the trace store
+};
+constexpr int kMaxOffDiag = 8;   // n_off_diag accepted: 0 .. kMaxOffDiag
+cudaError_t launch_offdiag(const ModelView &m, const TraceView &t, const OffdiagArgs &a,
+                           DevFlags *flags, cudaStream_t s);
+cudaError_t launch_jeff_nonlocal(const ModelView &m, const LevelArgs &a, const NonlocalArgs &nl,
+                                 cudaStream_t s);
+// prev3 <- prev2 <- prev1 <- pop for every cell
+cudaError_t launch_history_shift(const ModelView &m, const LevelArgs &a, cudaStream_t s);
+int nonlocal_sweep_blocks(const ModelView &m);
+// One block-Jacobi sweep x_in -> x_out and the max change into
+// change[nonlocal_sweep_blocks].
+cudaError_t launch_stateq_nonlocal_sweep(const ModelView &m, const LevelArgs &a,
+                                         const NonlocalArgs &nl, DevFlags *flags, cudaStream_t s);
 constexpr int kCellsPerPartial = 4;   // cells per convergence partial of launch_stateq
 cudaError_t launch_convergence(const ModelView &m, const LevelArgs &a, cudaStream_t s);
 cudaError_t launch_ng(const ModelView &m, const LevelArgs &a, cudaStream_t s);

@@ -286,7 +286,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
         const auto p = pol.load(ofr + nfr - 1);
         pol.eval_pt(m, p, b, chi, t);
         fr.chi_a = chi; fr.t_a = t; fr.dz_a = Pol::dz_of(p);
-        I0 = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
+        I0 = boundary_intensity(bc, pol.freq(p, b), p.cell, flags, b.k);
     }
     if (nfr >= 2) {
         const auto p = pol.load(ofr + nfr - 2);
@@ -300,7 +300,7 @@ __device__ __forceinline__ void sweep(const ModelView &m, const Pol &pol, const 
         const auto p = pol.load(obk + nbk - 1);
         pol.eval_pt(m, p, b, chi, t);
         bk.chi_a = chi; bk.t_a = t; bk.dz_a = Pol::dz_of(p);
-        In = boundary_intensity(bc, pol.freq(p, b), p.cell, flags);
+        In = boundary_intensity(bc, pol.freq(p, b), p.cell, flags, b.k);
         if (nbk >= 2) {
             const auto q = pol.load(obk + nbk - 2);
             pol.eval_pt(m, q, b, chi, t);
@@ -642,11 +642,11 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
     if (s == 0) {
         staged_eval<kCheck>(F, eo, q, floor_hat, chi, t_);
         fr.start(chi, t_, F->dzh);
-        I0 = boundary_intensity(bc, (1.0 + (double)F->delta) * b.nu_o, F->cell, flags);
+        I0 = boundary_intensity(bc, (1.0 + (double)F->delta) * b.nu_o, F->cell, flags, b.k);
         if (nbk > 0) {
             staged_eval<kCheck>(B, eo, q, floor_hat, chi, t_);
             bk.start(chi, t_, B->dzh);
-            In = boundary_intensity(bc, (1.0 + (double)B->delta) * b.nu_o, B->cell, flags);
+            In = boundary_intensity(bc, (1.0 + (double)B->delta) * b.nu_o, B->cell, flags, b.k);
         }
         s = 1;
     }
@@ -810,6 +810,7 @@ constexpr int kStageSteps64 = 32;
 struct Lane64 {
     double nu_o, line, inv_line;
     int eo;   // 0 or 2: this lane's line in StagedPt64::e
+    int k;    // this lane's line
 };
 
 __device__ __forceinline__ void staged_eval64(const StagedPt64 *p, const Lane64 &l, double &chi,
@@ -836,11 +837,11 @@ __device__ __forceinline__ void staged_window64(const StagedPt64 *F, const Stage
     if (s == 0) {
         staged_eval64(F, ln, chi, t_);
         fr.start(chi, t_, F->dzq);
-        I0 = boundary_intensity(bc, F->shift * ln.nu_o, (int)F->cell, flags);
+        I0 = boundary_intensity(bc, F->shift * ln.nu_o, (int)F->cell, flags, ln.k);
         if (nbk > 0) {
             staged_eval64(B, ln, chi, t_);
             bk.start(chi, t_, B->dzq);
-            In = boundary_intensity(bc, B->shift * ln.nu_o, (int)B->cell, flags);
+            In = boundary_intensity(bc, B->shift * ln.nu_o, (int)B->cell, flags, ln.k);
         }
         s = 1;
     }
@@ -999,6 +1000,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
         ln.line = line_k;
         ln.inv_line = m.inv_line[b.k];
         ln.eo = b.k != k0 ? 2 : 0;
+        ln.k = b.k;
         const double width_o = line_k * pw_o;
         const double iw = 1.0 / width_o;
         const double xo = iw * (b.nu_o - line_k);

@@ -40,6 +40,7 @@ class Simulation:
         self._h = h
         self.device = device
         self.model = None
+        self.n_off_diag = 0
         self.error_max = []
         self.error_mean = []
         self.fraction_not_converged = []
@@ -244,6 +245,27 @@ class Simulation:
         a, b = C.c_int64(0), C.c_int64(0)
         self._ck(self._lib.mgr_get_patch_stats(self._h, C.byref(a), C.byref(b)))
         return int(a.value), int(b.value)
+
+    def set_n_off_diag(self, n_off_diag: int):
+        """``parameters.n_off_diag``: 0 or 1 keep the diagonal ALO; M >= 2
+        keep the M-1 nearest off-diagonal elements on each side of every ray
+        pair and solve the rate equations of all cells as one system."""
+        self._ck(self._lib.mgr_set_n_off_diag(self._h, int(n_off_diag)))
+        self.n_off_diag = int(n_off_diag)
+
+    def alo_nonlocal(self):
+        """The off-diagonal ALO elements of the last formal solve:
+        (Loff [N, nrad, nrays/2, 2, M-1], Loff_nr [N, nrays/2, 2, M-1])."""
+        m, M1 = self.model, self.n_off_diag - 1
+        Loff = np.zeros((m.ncells, m.nlines, m.nrays // 2, 2, M1))
+        nr = np.zeros((m.ncells, m.nrays // 2, 2, M1), dtype=np.int64)
+        self._ck(self._lib.mgr_get_alo_nonlocal(self._h, _capi.ptr(Loff), _capi.ptr(nr)))
+        return Loff, nr
+
+    def nonlocal_sweeps(self) -> int:
+        n = C.c_int64()
+        self._ck(self._lib.mgr_get_nonlocal_sweeps(self._h, C.byref(n)))
+        return n.value
 
     def set_patch_capacity(self, entries: int):
         """Capacity of the mixed solve's list of solves redone in double

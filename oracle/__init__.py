@@ -46,7 +46,8 @@ class _State(C.Structure):
                 ("appears", _P), ("I_bdy", _P), ("pop", _P), ("prev1", _P), ("prev2", _P),
                 ("prev3", _P), ("emissivity", _P), ("opacity", _P), ("J", _P), ("Ls", _P),
                 ("Jlin", _P), ("Jeff", _P), ("Jdif", _P), ("fnc", _dbl), ("rcm", _dbl),
-                ("max_rel", _dbl), ("trace_errors", _i64), ("lu_errors", _i64)]
+                ("max_rel", _dbl), ("trace_errors", _i64), ("lu_errors", _i64),
+                ("n_off_diag", _i64), ("Loff", _P), ("Loff_nr", _P)]
 
 
 def build(force: bool = False) -> str:
@@ -92,6 +93,8 @@ def lib():
         L.orc_image_discretisation.argtypes = [_P, _P, _dbl]
         L.orc_compute_image.restype = C.c_int
         L.orc_compute_image.argtypes = [_P, _P, _P, _i64, _P, _P, C.c_int]
+        L.orc_raypair_lambda_row.restype = None
+        L.orc_raypair_lambda_row.argtypes = [_i64, _i64, _P, _P, _i64, _P, _P, _P]
         L.orc_compute_level_populations.restype = _i64
         L.orc_compute_level_populations.argtypes = [_P, _P, _P, C.c_int, _i64, _dbl, C.c_int, _P]
         _lib = L
@@ -111,6 +114,19 @@ def solve_raypair(n_ar: int, term1: np.ndarray, dtau: np.ndarray, I0: float, In:
     L = np.zeros(1)
     lib().orc_solve_raypair(n_ar, term1.shape[0], _ptr(term1), _ptr(dtau), I0, In, _ptr(u), _ptr(L))
     return float(u[0]), float(L[0])
+
+
+def raypair_lambda_row(n_ar: int, term1: np.ndarray, dtau: np.ndarray, n_off_diag: int):
+    """The origin's row of one ray pair's Lambda operator from the non-local
+    branch of RayPair::solve: (diagonal, [n_off_diag-1] elements toward the
+    front, [n_off_diag-1] toward the back)."""
+    term1 = np.ascontiguousarray(term1, dtype=np.float64)
+    dtau = np.ascontiguousarray(dtau, dtype=np.float64)
+    n = max(1, n_off_diag - 1)
+    diag, lo, up = np.zeros(1), np.zeros(n), np.zeros(n)
+    lib().orc_raypair_lambda_row(n_ar, term1.shape[0], _ptr(term1), _ptr(dtau), n_off_diag,
+                                 _ptr(diag), _ptr(lo), _ptr(up))
+    return float(diag[0]), lo[:n_off_diag - 1], up[:n_off_diag - 1]
 
 
 class Oracle:
@@ -227,6 +243,23 @@ class Oracle:
         lib().orc_lte(self.M, self.S)
         lib().orc_set_emissivity_opacity(self.M, self.S)
         return 0
+
+    def set_n_off_diag(self, n_off_diag: int):
+        """parameters.n_off_diag: with M >= 2 the formal solve also keeps the
+        M-1 nearest off-diagonal ALO elements on each side of every ray pair
+        (``Loff`` [N, nrad, npairs, 2, M-1] and their cells ``Loff_nr``
+        [N, npairs, 2, M-1], -1 where the pair has no such point), and the
+        statistical equilibrium solves the rate equations of all cells as one
+        system."""
+        m = self.m
+        M1 = max(0, int(n_off_diag) - 1)
+        np_ = m.nrays // 2
+        self.Loff = np.zeros((m.ncells, m.nlines, np_, 2, max(M1, 1)))
+        self.Loff_nr = np.full((m.ncells, np_, 2, max(M1, 1)), -1, dtype=np.int64)
+        self._state.n_off_diag = int(n_off_diag)
+        self._state.Loff = _ptr(self.Loff)
+        self._state.Loff_nr = _ptr(self.Loff_nr)
+        return self
 
     def setup(self):
         self.compute_spectral_discretisation()

@@ -345,7 +345,7 @@ void orc_set_emissivity_opacity(const orc_model *m, orc_state *s)
 typedef struct {
     int64_t cap;
     double *term1, *dtau, *chi, *frs, *A, *C, *F, *G, *Su;
-    double *inv_A, *inv_C, *inv1pF, *GoG;
+    double *inv_A, *inv_C, *inv1pF, *GoG, *inv1pG, *Ld;
     int64_t *nrs, *notch;
 } raypair_buf;
 
@@ -357,7 +357,8 @@ static void rp_ensure(raypair_buf *b, int64_t n)
     RP_GROW(term1, double); RP_GROW(dtau, double); RP_GROW(chi, double); RP_GROW(frs, double);
     RP_GROW(A, double); RP_GROW(C, double); RP_GROW(F, double); RP_GROW(G, double);
     RP_GROW(Su, double); RP_GROW(inv_A, double); RP_GROW(inv_C, double);
-    RP_GROW(inv1pF, double); RP_GROW(GoG, double); RP_GROW(nrs, int64_t); RP_GROW(notch, int64_t);
+    RP_GROW(inv1pF, double); RP_GROW(GoG, double); RP_GROW(inv1pG, double); RP_GROW(Ld, double);
+    RP_GROW(nrs, int64_t); RP_GROW(notch, int64_t);
 #undef RP_GROW
     b->cap = c;
 }
@@ -366,7 +367,7 @@ static void rp_free(raypair_buf *b)
 {
     free(b->term1); free(b->dtau); free(b->chi); free(b->frs); free(b->A); free(b->C);
     free(b->F); free(b->G); free(b->Su); free(b->inv_A); free(b->inv_C); free(b->inv1pF);
-    free(b->GoG); free(b->nrs); free(b->notch);
+    free(b->GoG); free(b->inv1pG); free(b->Ld); free(b->nrs); free(b->notch);
 }
 
 /* RayPair::solve, Simulation/Raypair/raypair_solver.tpp:200-334 (the
@@ -426,6 +427,89 @@ static void solve_raypair(raypair_buf *b, int64_t first, int64_t last, int64_t n
     }
 }
 
+/* RayPair::solve with n_off_diag > 0 (raypair_solver.tpp:336-388): the
+ * same elimination, back substitution over the whole pair, and the diagonal
+ * of the ray pair's Lambda operator at every point (Ld) with the factors
+ * 1/(1+F) and 1/(1+G) its off-diagonal elements are built from. */
+static void solve_raypair_nonlocal(raypair_buf *b, int64_t first, int64_t last, int64_t n_ar,
+                                   double I_bdy_0, double I_bdy_n, double *u, double *L)
+{
+    double *A = b->A, *C = b->C, *F = b->F, *G = b->G, *Su = b->Su, *dtau = b->dtau;
+    double *inv_A = b->inv_A, *inv_C = b->inv_C, *inv1pF = b->inv1pF, *inv1pG = b->inv1pG;
+    double *Ld = b->Ld;
+    const double *term1 = b->term1;
+
+    const double inverse_dtau0 = 1.0 / dtau[first];
+    const double inverse_dtaud = 1.0 / dtau[last - 1];
+    C[first] = 2.0 * inverse_dtau0 * inverse_dtau0;
+    const double B0_min_C0 = 1.0 + 2.0 * inverse_dtau0;
+    const double B0 = B0_min_C0 + C[first];
+    const double inverse_B0 = 1.0 / B0;
+    Su[first] = term1[first] + 2.0 * I_bdy_0 * inverse_dtau0;
+    for (int64_t n = first + 1; n < last; n++) {
+        inv_A[n] = 0.5 * (dtau[n - 1] + dtau[n]) * dtau[n - 1];
+        A[n] = 1.0 / inv_A[n];
+        inv_C[n] = 0.5 * (dtau[n - 1] + dtau[n]) * dtau[n];
+        C[n] = 1.0 / inv_C[n];
+        Su[n] = term1[n];
+    }
+    A[last] = 2.0 * inverse_dtaud * inverse_dtaud;
+    const double Bd_min_Ad = 1.0 + 2.0 * inverse_dtaud;
+    const double Bd = Bd_min_Ad + A[last];
+    Su[last] = term1[last] + 2.0 * I_bdy_n * inverse_dtaud;
+
+    Su[first] = Su[first] * inverse_B0;
+    F[first] = 0.5 * B0_min_C0 * dtau[first] * dtau[first];
+    inv1pF[first] = 1.0 / (1.0 + F[first]);
+    for (int64_t n = first + 1; n < last; n++) {
+        F[n] = (1.0 + A[n] * F[n - 1] * inv1pF[n - 1]) * inv_C[n];
+        inv1pF[n] = 1.0 / (1.0 + F[n]);
+        Su[n] = (Su[n] + A[n] * Su[n - 1]) * inv1pF[n] * inv_C[n];
+    }
+    const double denominator = 1.0 / (Bd_min_Ad + Bd * F[last - 1]);
+    Su[last] = (Su[last] + A[last] * Su[last - 1]) * (1.0 + F[last - 1]) * denominator;
+
+    G[last] = 0.5 * Bd_min_Ad * dtau[last - 1] * dtau[last - 1];
+    inv1pG[last] = 1.0 / (1.0 + G[last]);
+    for (int64_t n = last - 1; n > first; n--) {
+        Su[n] = Su[n] + Su[n + 1] * inv1pF[n];
+        G[n] = (1.0 + C[n] * G[n + 1] * inv1pG[n + 1]) * inv_A[n];
+        inv1pG[n] = 1.0 / (1.0 + G[n]);
+    }
+    Su[first] = Su[first] + Su[first + 1] * inv1pF[first];
+
+    Ld[last] = (1.0 + F[last - 1]) / (Bd_min_Ad + Bd * F[last - 1]);
+    for (int64_t n = last - 1; n >= first + 1; n--)
+        Ld[n] = inv_C[n] / (F[n] + G[n + 1] * inv1pG[n + 1]);
+    Ld[first] = (1.0 + G[first + 1]) / (B0_min_C0 + B0 * G[first + 1]);
+    *u = Su[n_ar];
+    *L = Ld[n_ar];
+}
+
+/* Element (n_ar, n_ar - d) and (n_ar, n_ar + d) of the ray pair's Lambda
+ * operator from the factors of solve_raypair_nonlocal, multiplied in the
+ * order of the reference's recursions (raypair_solver.tpp:372-388):
+ * L_lower[d-1][n_ar-d] = Ld[n_ar-d] * 1/(1+G[n_ar-d+1]) * ... * 1/(1+G[n_ar]),
+ * L_upper[d-1][n_ar]   = Ld[n_ar+d] * 1/(1+F[n_ar+d-1]) * ... * 1/(1+F[n_ar]).
+ * These are the origin's row.  RayPair::update_Lambda
+ * (raypair_lambda.tpp:129-145) reads L_lower[d][n_ar-d] and
+ * L_upper[d][n_ar+d] instead, the elements (n_ar+1, n_ar-d) and
+ * (n_ar+d, n_ar+2d+1), and at the ends of the pair (n_ar = last, or
+ * n_ar + 2d = last) entries its recursions did not write for this pair. */
+static inline double lambda_lower(const raypair_buf *b, int64_t n_ar, int64_t d)
+{
+    double lam = b->Ld[n_ar - d];
+    for (int64_t q = n_ar - d + 1; q <= n_ar; q++) lam *= b->inv1pG[q];
+    return lam;
+}
+
+static inline double lambda_upper(const raypair_buf *b, int64_t n_ar, int64_t d)
+{
+    double lam = b->Ld[n_ar + d];
+    for (int64_t q = n_ar + d - 1; q >= n_ar; q--) lam *= b->inv1pF[q];
+    return lam;
+}
+
 void orc_solve_raypair(int64_t n_ar, int64_t ndep, const double *term1, const double *dtau,
                        double I_bdy_0, double I_bdy_n, double *u_origin, double *L_origin)
 {
@@ -435,6 +519,23 @@ void orc_solve_raypair(int64_t n_ar, int64_t ndep, const double *term1, const do
     memcpy(b.term1, term1, sizeof(double) * (size_t)ndep);
     memcpy(b.dtau, dtau, sizeof(double) * (size_t)(ndep - 1));
     solve_raypair(&b, 0, ndep - 1, n_ar, I_bdy_0, I_bdy_n, u_origin, L_origin);
+    rp_free(&b);
+}
+
+void orc_raypair_lambda_row(int64_t n_ar, int64_t ndep, const double *term1, const double *dtau,
+                            int64_t n_off_diag, double *diag, double *lower, double *upper)
+{
+    raypair_buf b;
+    memset(&b, 0, sizeof(b));
+    rp_ensure(&b, ndep + 1);
+    memcpy(b.term1, term1, sizeof(double) * (size_t)ndep);
+    memcpy(b.dtau, dtau, sizeof(double) * (size_t)(ndep - 1));
+    double u;
+    solve_raypair_nonlocal(&b, 0, ndep - 1, n_ar, 0.0, 0.0, &u, diag);
+    for (int64_t d = 1; d < n_off_diag; d++) {
+        lower[d - 1] = n_ar - d >= 0 ? lambda_lower(&b, n_ar, d) : 0.0;
+        upper[d - 1] = n_ar + d <= ndep - 1 ? lambda_upper(&b, n_ar, d) : 0.0;
+    }
     rp_free(&b);
 }
 
@@ -585,13 +686,23 @@ static void solve_origin_pair(const orc_model *m, orc_state *s, const line_table
         rp_ensure(rb, ndep + 1);
         int64_t lnotch_at_origin = 0;                      /* RayPair::initialize */
         for (int64_t i = 0; i < ndep; i++) rb->notch[i] = 0;  /* ProjectedCellData.lnotch */
+        if (s->n_off_diag > 1) {
+            const int64_t M1 = s->n_off_diag - 1, np = m->nrays / 2;
+            for (int64_t d = 1; d <= M1; d++) {
+                s->Loff_nr[((o * np + r) * 2 + 0) * M1 + d - 1] = d <= n_ar ? front->cell[d - 1] : -1;
+                s->Loff_nr[((o * np + r) * 2 + 1) * M1 + d - 1] = d <= n_r ? back->cell[d - 1] : -1;
+            }
+        }
         for (int64_t f = 0; f < nf; f++) {
             double I_bdy_0, I_bdy_n;
             int64_t first, last;
             setup_pair(m, s, lt, o, f, front, back, rb, &lnotch_at_origin, &first, &last,
                        &I_bdy_0, &I_bdy_n);
             double u, Ld;
-            solve_raypair(rb, first, last, n_ar, I_bdy_0, I_bdy_n, &u, &Ld);
+            if (s->n_off_diag > 0)
+                solve_raypair_nonlocal(rb, first, last, n_ar, I_bdy_0, I_bdy_n, &u, &Ld);
+            else
+                solve_raypair(rb, first, last, n_ar, I_bdy_0, I_bdy_n, &u, &Ld);
             if (s->appears[f]) {
                 const int64_t k = s->corr_k[f], z = s->corr_z[f];
                 const double freq_line = m->frequency[k];
@@ -601,6 +712,21 @@ static void solve_origin_pair(const orc_model *m, orc_state *s, const line_table
                                             rb->frs[n_ar] - freq_line);
                 const double L = factor * (rb->frs[n_ar] * prof * Ld / rb->chi[n_ar]);
                 s->Ls[o * m->nrad + k] += L;
+                /* off-diagonal elements (raypair_lambda.tpp:129-145 with the
+                 * origin's row, see lambda_lower) */
+                const int64_t M1 = s->n_off_diag - 1, np = m->nrays / 2;
+                for (int64_t d = 1; d <= M1; d++) {
+                    for (int side = 0; side < 2; side++) {
+                        const int64_t j = side == 0 ? n_ar - d : n_ar + d;
+                        if (j < first || j > last) continue;
+                        const double lam = side == 0 ? lambda_lower(rb, n_ar, d)
+                                                     : lambda_upper(rb, n_ar, d);
+                        const double pj = profile(freq_line * profile_width(m, rb->nrs[j]),
+                                                  rb->frs[j] - freq_line);
+                        const double Lj = factor * (rb->frs[j] * pj * lam / rb->chi[j]);
+                        s->Loff[(((o * m->nrad + k) * np + r) * 2 + side) * M1 + d - 1] += Lj;
+                    }
+                }
             }
             s->J[o * nf + f] += 2.0 * weight_ang * u;
         }
@@ -609,6 +735,10 @@ static void solve_origin_pair(const orc_model *m, orc_state *s, const line_table
         for (int64_t f = 0; f < nf; f++) {
             const double u = 0.5 * (s->I_bdy[b * nf + f] + s->I_bdy[b * nf + f]);
             s->J[o * nf + f] += 2.0 * weight_ang * u;
+        }
+        if (s->n_off_diag > 1) {
+            const int64_t M1 = s->n_off_diag - 1, np = m->nrays / 2;
+            for (int64_t i = 0; i < 2 * M1; i++) s->Loff_nr[(o * np + r) * 2 * M1 + i] = -1;
         }
     }
 }
@@ -636,6 +766,10 @@ int orc_compute_radiation_field(const orc_model *m, orc_state *s, const int64_t 
         const int64_t o = origins ? origins[i] : i;
         memset(s->J + o * nf, 0, sizeof(double) * (size_t)nf);
         memset(s->Ls + o * m->nrad, 0, sizeof(double) * (size_t)m->nrad);
+        if (s->n_off_diag > 1) {
+            const int64_t per = m->nrad * (m->nrays / 2) * 2 * (s->n_off_diag - 1);
+            memset(s->Loff + o * per, 0, sizeof(double) * (size_t)per);
+        }
     }
     int64_t errs = 0;
     for (int64_t r = 0; r < np; r++) {
@@ -1039,6 +1173,16 @@ void orc_compute_jeff(const orc_model *m, orc_state *s)
                 jl += m->quad_weights[z] * s->J[p * nf + s->nr_line[p * nf + k * nq + z]];
             double diff = 0.0;
             diff += s->Ls[p * nr + k] * s->pop[p * nl + m->irad[k]];
+            if (s->n_off_diag > 1) {   /* the non-local elements of (p, k) */
+                const int64_t M1 = s->n_off_diag - 1, np = m->nrays / 2;
+                for (int64_t r = 0; r < np; r++)
+                    for (int64_t i = 0; i < 2 * M1; i++) {
+                        const int64_t c = s->Loff_nr[(p * np + r) * 2 * M1 + i];
+                        if (c < 0) continue;
+                        diff += s->Loff[((p * nr + k) * np + r) * 2 * M1 + i] *
+                                s->pop[c * nl + m->irad[k]];
+                    }
+            }
             s->Jlin[p * nr + k] = jl;
             s->Jeff[p * nr + k] = jl - O_HH_OVER_FOUR_PI * diff;
             s->Jdif[p * nr + k] = O_HH_OVER_FOUR_PI * diff;
@@ -1112,6 +1256,139 @@ static int lu_solve(int64_t n, double *M, double *y)
     return 0;
 }
 
+/* Collision rates of cell p into the rows of cell block `base` of a dense
+ * matrix with leading dimension ld (lineProducingSpecies.tpp:344-378). */
+static void add_collisions(const orc_model *m, int64_t p, double *Mrow0, int64_t ld,
+                           int64_t base, double *Cd_i, double *Ce_i)
+{
+    const int64_t last = m->nlev - 1;
+    for (int c = 0; c < m->ncolpar; c++) {
+        const orc_colpar *cp = &m->colpar[c];
+        double abn = cp->abundance[p];
+        const double tmp = m->temperature[p];
+        if (cp->ortho_para != 0) {
+            const double frac_H2_para = 1.0 / (1.0 + 9.0 * exp(-170.5 / tmp));
+            if (cp->ortho_para == 1) abn *= (1.0 - frac_H2_para);
+            if (cp->ortho_para == 2) abn *= frac_H2_para;
+        }
+        interpolate_collision(cp, tmp, Cd_i, Ce_i);
+        for (int64_t k = 0; k < cp->ncol; k++) {
+            const double v_IJ = Cd_i[k] * abn;
+            const double v_JI = Ce_i[k] * abn;
+            const int64_t I = base + cp->icol[k], J = base + cp->jcol[k];
+            if (cp->jcol[k] != last) { Mrow0[J * ld + I] += +v_IJ; Mrow0[J * ld + J] += -v_JI; }
+            if (cp->icol[k] != last) { Mrow0[I * ld + J] += +v_JI; Mrow0[I * ld + I] += -v_IJ; }
+        }
+    }
+}
+
+/* update_using_statistical_equilibrium with a non-local ALO (n_off_diag >= 2,
+ * lineProducingSpecies.tpp:249-495).  The cell blocks hold the reference's
+ * triplets in its order -- radiative rates, then for each line the ALO
+ * elements (nr, Ls) of the cell with v = -Ls * opacity(p, k), then
+ * collisions, then the conservation row.  An element couples the rows of
+ * cell p's lower and upper levels to the upper level of cell nr: v at
+ * (J(p), I(nr)) and -v at (I(p), I(nr)), the terms that cancel the
+ * element's part of Jeff once the populations stop changing.  (The
+ * reference writes the second at (I(nr), I(nr)) (lineProducingSpecies.tpp:
+ * 325-338), the same place when nr = p; for nr != p that leaves
+ * -Ls*opacity*n_I(nr) uncancelled in cell p's upper-level row and moves the
+ * converged populations.)  Elements with nr = p go into p's block; the
+ * others couple the blocks.  The global system (SparseLU<COLAMD> there) is
+ * solved by block Jacobi: each cell's block by partial-pivot LU with the
+ * couplings to the other cells' current populations moved to the right-hand
+ * side, from the populations before the solve, until no population changes
+ * by more than 1e-14 of itself (of 1e-10 of the cell's total for the levels
+ * below that, which the convergence test ignores), or, once below 1e-8, the
+ * change has set no new low for three sweeps (the rounding floor of the cell
+ * solves); at most 1000 sweeps, a sweep count past that is an error.  Solving cell by cell keeps every block's own scaling,
+ * which a dense LU of the whole model (populations over 10 orders of
+ * magnitude) loses for the weakly populated levels. */
+static int statistical_equilibrium_global(const orc_model *m, orc_state *s)
+{
+    const int64_t nl = m->nlev, nr = m->nrad, N = m->ncells, n = N * nl;
+    const int64_t M1 = s->n_off_diag - 1, np = m->nrays / 2, ne = np * 2 * M1;
+    memcpy(s->prev3, s->prev2, sizeof(double) * (size_t)n);
+    memcpy(s->prev2, s->prev1, sizeof(double) * (size_t)n);
+    memcpy(s->prev1, s->pop, sizeof(double) * (size_t)n);
+    double *xa = (double *)malloc(sizeof(double) * (size_t)n);
+    double *xb = (double *)malloc(sizeof(double) * (size_t)n);
+    memcpy(xa, s->prev1, sizeof(double) * (size_t)n);
+    double *B = (double *)malloc(sizeof(double) * (size_t)(nl * nl));
+    double *y = (double *)malloc(sizeof(double) * (size_t)nl);
+    int64_t maxcol = 1;
+    for (int c = 0; c < m->ncolpar; c++) if (m->colpar[c].ncol > maxcol) maxcol = m->colpar[c].ncol;
+    double *Cd_i = (double *)malloc(sizeof(double) * (size_t)maxcol);
+    double *Ce_i = (double *)malloc(sizeof(double) * (size_t)maxcol);
+    const int64_t last = nl - 1;
+    int bad = 0, sweep, best_sweep = 0;
+    double best = INFINITY;
+    for (sweep = 0; sweep < 1000 && !bad; sweep++) {
+        double change = 0.0;
+        for (int64_t p = 0; p < N && !bad; p++) {
+            const double *pop = s->prev1 + p * nl;
+            memset(B, 0, sizeof(double) * (size_t)(nl * nl));
+            memset(y, 0, sizeof(double) * (size_t)nl);
+            for (int64_t k = 0; k < nr; k++) {
+                const double Jeff = s->Jeff[p * nr + k];
+                const double v_IJ = m->A[k] + m->Bs[k] * Jeff;
+                const double v_JI = m->Ba[k] * Jeff;
+                const int64_t I = m->irad[k], J = m->jrad[k];
+                if (J != last) { B[J * nl + I] += +v_IJ; B[J * nl + J] += -v_JI; }
+                if (I != last) { B[I * nl + J] += +v_JI; B[I * nl + I] += -v_IJ; }
+            }
+            for (int64_t k = 0; k < nr; k++) {
+                const double opac = O_HH_OVER_FOUR_PI * (pop[m->jrad[k]] * m->Ba[k] - pop[m->irad[k]] * m->Bs[k]);
+                const int64_t I = m->irad[k], J = m->jrad[k];
+                for (int64_t e = -1; e < ne; e++) {
+                    int64_t c;
+                    double Ls;
+                    if (e < 0) {
+                        c = p;
+                        Ls = s->Ls[p * nr + k];
+                    } else {
+                        c = s->Loff_nr[p * ne + e];
+                        if (c < 0) continue;
+                        Ls = s->Loff[(p * nr + k) * ne + e];
+                    }
+                    const double v_IJ = -Ls * opac;
+                    if (c == p) {
+                        if (J != last) B[J * nl + I] += +v_IJ;
+                        if (I != last) B[I * nl + I] += -v_IJ;
+                    } else {
+                        const double xc = xa[c * nl + I];
+                        if (J != last) y[J] -= v_IJ * xc;
+                        if (I != last) y[I] += v_IJ * xc;
+                    }
+                }
+            }
+            add_collisions(m, p, B, nl, 0, Cd_i, Ce_i);
+            for (int64_t i = 0; i < nl; i++) B[last * nl + i] += 1.0;
+            y[last] = m->population_tot[p];
+            if (lu_solve(nl, B, y)) { bad = 1; break; }
+            /* change relative to the population, or to 1e-10 of the cell's
+             * total below it (the levels the convergence test ignores) */
+            const double floor_p = 1.0E-10 * m->population_tot[p];
+            for (int64_t i = 0; i < nl; i++) {
+                const double v = y[i];
+                const double d = fabs(v - xa[p * nl + i]) / fmax(fabs(v), floor_p);
+                if (d > change) change = d;
+                xb[p * nl + i] = v;
+            }
+        }
+        double *t = xa; xa = xb; xb = t;
+        if (change <= 1.0E-14) { sweep++; break; }
+        /* at the rounding floor of the cell solves: no new low in 3 sweeps */
+        if (change < best) { best = change; best_sweep = sweep; }
+        else if (best < 1.0E-8 && sweep >= best_sweep + 3) { sweep++; break; }
+    }
+    if (!bad && sweep >= 1000) bad = 2;
+    if (!bad) memcpy(s->pop, xa, sizeof(double) * (size_t)n);
+    s->lu_errors = bad ? 1 : 0;
+    free(xa); free(xb); free(B); free(y); free(Cd_i); free(Ce_i);
+    return bad;
+}
+
 /* LineProducingSpecies::update_using_statistical_equilibrium,
  * lineProducingSpecies.tpp:249-495.  With n_off_diag = 0 the rate matrix is
  * block diagonal; each cell's block is assembled from the same triplets in
@@ -1120,6 +1397,7 @@ static int lu_solve(int64_t n, double *M, double *y)
  * in place of SparseLU<COLAMD> (whose pivot order is not pinned here). */
 int orc_statistical_equilibrium(const orc_model *m, orc_state *s)
 {
+    if (s->n_off_diag > 1) return statistical_equilibrium_global(m, s);
     const int64_t nl = m->nlev, nr = m->nrad, N = m->ncells;
     memcpy(s->prev3, s->prev2, sizeof(double) * (size_t)(N * nl));
     memcpy(s->prev2, s->prev1, sizeof(double) * (size_t)(N * nl));

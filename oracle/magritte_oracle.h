@@ -101,6 +101,14 @@ typedef struct {
     double  max_rel;               /* max relative change over n > 1e-10 n_tot */
     int64_t trace_errors;
     int64_t lu_errors;
+    /* non-local ALO (parameters.n_off_diag = M >= 2; 0 or 1 leaves Loff
+     * unused): for origin o, line k, ray pair r, side (0 the front trace, 1
+     * the back trace) and distance d = 1..M-1 from the origin, the element
+     * Loff[(((o*nrad + k)*npairs + r)*2 + side)*(M-1) + d-1] of the cell
+     * Loff_nr[((o*npairs + r)*2 + side)*(M-1) + d-1] (-1: no such point) */
+    int64_t n_off_diag;
+    double  *Loff;
+    int64_t *Loff_nr;
 } orc_state;
 
 /* Constants, exposed so tests can reuse the reference's values. */
@@ -138,6 +146,12 @@ int orc_compute_radiation_field(const orc_model *m, orc_state *s, const int64_t 
 /* one ray pair: reference elimination + back substitution on given arrays */
 void orc_solve_raypair(int64_t n_ar, int64_t ndep, const double *term1, const double *dtau,
                        double I_bdy_0, double I_bdy_n, double *u_origin, double *L_origin);
+
+/* one ray pair, n_off_diag > 0: the diagonal element at the origin and the
+ * n_off_diag-1 elements of the origin's row on each side (0 where the pair
+ * has no such point) */
+void orc_raypair_lambda_row(int64_t n_ar, int64_t ndep, const double *term1, const double *dtau,
+                            int64_t n_off_diag, double *diag, double *lower, double *upper);
 
 /* level populations */
 void orc_compute_jeff(const orc_model *m, orc_state *s);

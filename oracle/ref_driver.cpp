@@ -45,6 +45,8 @@
 //                                              time each; then J, Jlin, Jeff,
 //                                              ALO as for radiation
 //
+// MGR_REF_N_OFF_DIAG=<M> sets parameters.n_off_diag before anything runs.
+//
 // The call sequence follows the reference's examples
 // (src/examples/example_1.cpp: read, compute_spectral_discretisation,
 // compute_boundary_intensities, compute_LTE_level_populations, ...), with
@@ -125,6 +127,8 @@ int main(int argc, char **argv) {
     IoText io(model);
     Simulation sim;
     sim.read(io);
+    // parameters.n_off_diag (a plain member, not part of the model folder)
+    if (const char *noff = std::getenv("MGR_REF_N_OFF_DIAG")) sim.parameters.n_off_diag = std::atol(noff);
     if (cmd == "radiation") {
         const bool lte = !(argc > 4 && std::string(argv[4]) == "--pops");
         set_up(sim, lte);
