@@ -45,7 +45,10 @@ bool flatten(const Simulation &sim, Flat &f, std::string &why) {
     const Linedata &ld = ls.linedata;
     const long N = (long)sim.parameters.ncells();
     if (sim.parameters.nlspecs() != 1) { why = "one line-producing species"; return false; }
-    if (sim.parameters.n_off_diag != 0) { why = "n_off_diag = 0 (local ALO)"; return false; }
+    if (sim.parameters.n_off_diag < 0 || sim.parameters.n_off_diag > 8) {
+        why = "n_off_diag in 0 .. 8";
+        return false;
+    }
     f.pos.resize(3 * N);
     f.vel.resize(3 * N);
     f.off.assign(N + 1, 0);
@@ -145,6 +148,7 @@ mgr_handle *open(Simulation &sim, int device, Flat &f, std::string &why) {
     mgr_handle *h = nullptr;
     if (mgr_create(device, &h) != MGR_OK) { why = "no CUDA device"; return nullptr; }
     mgr_status s = mgr_upload_model(h, &f.d);
+    if (s == MGR_OK) s = mgr_set_n_off_diag(h, (int32_t)sim.parameters.n_off_diag);
     if (s == MGR_OK) s = mgr_compute_spectral_discretisation(h);
     if (s == MGR_OK) s = mgr_compute_boundary_intensities(h);
     if (s == MGR_OK) s = mgr_set_populations(h, sim.lines.lineProducingSpecies[0].population.data());

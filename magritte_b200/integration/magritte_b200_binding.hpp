@@ -5,7 +5,8 @@
 // leaves it after read(), compute_spectral_discretisation(),
 // compute_boundary_intensities() and a start for the populations
 // (compute_LTE_level_populations() or populations read from a model), and
-// leave their results in its containers.
+// leave their results in its containers.  parameters.n_off_diag is honoured
+// (0 .. 8; 2 and more: the non-local ALO of mgr_set_n_off_diag).
 #pragma once
 
 #include "Simulation/simulation.hpp"
