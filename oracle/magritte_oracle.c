@@ -1299,8 +1299,8 @@ static void add_collisions(const orc_model *m, int64_t p, double *Mrow0, int64_t
  * couplings to the other cells' current populations moved to the right-hand
  * side, from the populations before the solve, until no population changes
  * by more than 1e-14 of itself (of 1e-10 of the cell's total for the levels
- * below that, which the convergence test ignores), or, once below 1e-8, the
- * change has set no new low for three sweeps (the rounding floor of the cell
+ * below that, which the convergence test ignores), or, once below 1e-6, the
+ * change has set no new low for five sweeps (the rounding floor of the cell
  * solves); at most 1000 sweeps, a sweep count past that is an error.  Solving cell by cell keeps every block's own scaling,
  * which a dense LU of the whole model (populations over 10 orders of
  * magnitude) loses for the weakly populated levels. */
@@ -1378,9 +1378,9 @@ static int statistical_equilibrium_global(const orc_model *m, orc_state *s)
         }
         double *t = xa; xa = xb; xb = t;
         if (change <= 1.0E-14) { sweep++; break; }
-        /* at the rounding floor of the cell solves: no new low in 3 sweeps */
+        /* at the rounding floor of the cell solves: no new low in 5 sweeps */
         if (change < best) { best = change; best_sweep = sweep; }
-        else if (best < 1.0E-8 && sweep >= best_sweep + 3) { sweep++; break; }
+        else if (best < 1.0E-6 && sweep >= best_sweep + 5) { sweep++; break; }
     }
     if (!bad && sweep >= 1000) bad = 2;
     if (!bad) memcpy(s->pop, xa, sizeof(double) * (size_t)n);
