@@ -482,11 +482,13 @@ def run_b200(args):
         import torch.distributed as tdist
         torch.cuda.set_device(local)
         if dist:
-            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            # a rank that loses its peers ends its next collective with an
+            # error within 5 minutes (a formal solve here takes seconds)
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         else:
             tdist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{free_port()}",
                                      rank=0, world_size=1,
-                                     timeout=datetime.timedelta(seconds=600))
+                                     timeout=datetime.timedelta(seconds=300))
     model = make_model(args.workload)
     prec = args.precision
     net = None
