@@ -573,7 +573,7 @@ def run_b200(args):
         model_iters = {"min": int(mit.min()), "median": float(np.median(mit)),
                        "max": int(mit.max()), "sum": int(mit.sum()),
                        "not_converged": [int(i) for i in np.nonzero(~(mst[:, 2] < TOL))[0]]}
-    tuning = sim.tuning(prec) if not args.no_autotune else None
+    tuning = sim.tuning(prec)   # the kernel that ran (and, with the autotuner, its timings)
     err_hist = list(sim.error_max)
     t_step = statistics.mean(times)
 

@@ -191,8 +191,8 @@ __device__ __forceinline__ BdyCtx bdy_ctx(const ModelView &m) {
 // bisection), then the bin within that line, from a guess on the root grid
 // walked up or down to the first bin >= freq (two checks when the guess is
 // right, which on an evenly spaced root grid it is but for rounding).
-static __device__ __noinline__ double boundary_intensity(BdyCtx c, double freq, int p,
-                                                         DevFlags *flags, int k_hint = -1) {
+static __device__ __forceinline__ double boundary_intensity(BdyCtx c, double freq, int p,
+                                                            DevFlags *flags, int k_hint = -1) {
     const int b = __ldg(c.cell2bdy + p);
     if (b < 0) {
         atomicAdd(&flags->trace_err, 1ull);
