@@ -494,16 +494,23 @@ def turbulent_cloud(n: int = 128, L: float = 1.0e14, seed: int = 5, nlev: int = 
 
 
 def slab_1d(n: int = 50, L: float = 1.0e13, n_h2: float = 1.0e12, x_abund: float = 1.0e-6,
-            T: float = 250.0, vturb: float = 250.0, nquads: int = 31) -> Model:
+            T: float = 250.0, vturb: float = 250.0, nquads: int = 31,
+            vmax: float = 0.0) -> Model:
     """Constant 1D slab with rays +x and -x (weights 1/2), the set-up whose
     mean intensity has the closed form J = S + (B-S)/2 (e^-tau(x) + e^-tau(L-x))
-    (``tests/integration/test_0_1D_all_constant.py:240-244``)."""
+    (``tests/integration/test_0_1D_all_constant.py:240-244``).  With vmax
+    (m/s) the velocity rises linearly along x from 0 to vmax, the set-up of
+    ``tests/integration/test_1_1D_velocity_gradient.py``, where tau follows
+    from the shifted profile as a difference of error functions."""
     pos, offs, nbr, b2c = chain_grid(n, L)
     rays = np.array([[1.0, 0.0, 0.0], [-1.0, 0.0, 0.0]])
     w = np.array([0.5, 0.5])
-    return _assemble(pos, offs, nbr, b2c, np.zeros((n, 3)), T, vturb, np.full(n, n_h2),
-                     x_abund, two_level_species(), rays, w, nquads, f"slab_{n}",
-                     dict(kind="slab", n=n, L=L))
+    vel = np.zeros((n, 3))
+    vel[:, 0] = vmax * pos[:, 0] / L / CC
+    return _assemble(pos, offs, nbr, b2c, vel, T, vturb, np.full(n, n_h2),
+                     x_abund, two_level_species(), rays, w, nquads,
+                     f"slab_{n}" if vmax == 0.0 else f"slab_{n}_gradient",
+                     dict(kind="slab", n=n, L=L, vmax=vmax))
 
 
 # ----------------------------------------------------------- named configs

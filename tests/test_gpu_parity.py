@@ -82,7 +82,8 @@ def test_npoints_on_rays(gpu):
     assert np.array_equal(sim.get_npoints_on_rays(), orc.get_npoints_on_rays())
 
 
-@pytest.mark.parametrize("make", [M.config1, lambda: small_wind(10, 5, 7), M.config3])
+@pytest.mark.parametrize("make", [M.config1, lambda: small_wind(10, 5, 7), M.config3,
+                                  lambda: M.slab_1d(100, x_abund=1e-4, vmax=980.0)])
 def test_radiation_field_fp64(gpu, make):
     model = make()
     sim, orc = setup_pair(model)

@@ -159,6 +159,46 @@ def _slab_error(n, x_abund):
     return float(np.max(np.abs(o.J - J) / J))
 
 
+def _gradient_slab_error(n, vmax, x_abund=1e-4):
+    """The slab with velocity rising linearly to vmax along x against the
+    closed form of tests/integration/test_1_1D_velocity_gradient.py: with
+    a = vmax/c, tau_nu(l) = kappa L nu / (a nu) * 1/2
+    (erf((nu - nu0)/dnu) + erf(a nu/dnu l/L - (nu - nu0)/dnu)) in each
+    direction, J = S + (B - S)/2 (e^-tau(x) + e^-tau(L - x))."""
+    from scipy.special import erf
+    m = M.slab_1d(n, x_abund=x_abund, vmax=vmax)
+    o = oracle.Oracle(m).setup()
+    o.compute_radiation_field()
+    ld = m.linedata
+    eps, kap = o.emissivity[0, 0], o.opacity[0, 0]
+    pw = math.sqrt(2 * M.KB / (M.AMU * M.C_SQUARED) * ld.inverse_mass * m.temperature[0]
+                   + m.vturb2[0])
+    nu0 = ld.frequency[0]
+    dnu = nu0 * pw
+    x = m.position[:, 0]
+    L = x[-1]
+    nu = o.nu[0][None, :]
+    fct = vmax / M.CC * nu / dnu
+    arg = (nu - nu0) / dnu
+
+    def tau(l):
+        return kap * L * nu / (fct * dnu) * 0.5 * (erf(arg) + erf(fct * l / L - arg))
+
+    S = eps / kap
+    B = o.I_bdy[0][None, :]
+    J = S + 0.5 * (B - S) * (np.exp(-tau(x[:, None])) + np.exp(-tau((L - x)[:, None])))
+    return float(np.max(np.abs(o.J - J) / J))
+
+
+def test_velocity_gradient_slab_analytic():
+    """J of the velocity-gradient slab (2 Doppler widths across) against the
+    closed form; second-order convergence as for the constant slab."""
+    e50 = _gradient_slab_error(50, 980.0)
+    e200 = _gradient_slab_error(200, 980.0)
+    assert e50 < 2e-3
+    assert e200 < e50 / 8.0
+
+
 @pytest.mark.parametrize("x_abund,tol50", [(1e-6, 1e-8), (1e-4, 1e-4), (1e-3, 1e-2)])
 def test_constant_slab_analytic(x_abund, tol50):
     """J of a constant slab against the closed form; the error falls as
