@@ -368,7 +368,9 @@ __global__ void __launch_bounds__(kStateqWarps * 32) stateq_nonlocal_kernel(Mode
         __syncwarp();
         const bool singular = warp_lu(M, y, nlev, i);
         if (singular) {
+            // the cell keeps its populations; the solve reports the zero pivot
             if (lane == 0) atomicAdd(&flags->lu_err, 1ull);
+            if (i < nlev) nl.x_out[p * nlev + i] = nl.x_in[p * nlev + i];
         } else {
             warp_back_substitute(M, y, nlev, i);
             if (i < nlev) {
