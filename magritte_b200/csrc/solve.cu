@@ -578,57 +578,6 @@ __device__ __forceinline__ void staged_eval(const StagedPt *p, int eo, float q, 
 }
 
 
-// Two staged points at once (the front and the back chain's next points,
-// or two consecutive points of one chain), the float arithmetic in packed
-// f32x2 instructions of sm_100a: each half is the same sequence of rounded
-// operations as staged_eval, so the results are identical; the packed form
-// issues half the FP32 instructions (1 % off the mixed solve on the 64^3
-// wind).
-__device__ __forceinline__ unsigned long long pk2(float a, float b) {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ void up2(unsigned long long v, float &a, float &b) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-}
-__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
-    unsigned long long d;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b) {
-    unsigned long long d;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
-}
-__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
-                                                   unsigned long long c) {
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-template <bool kCheck>
-__device__ __forceinline__ void staged_eval2(const StagedPt *pa, const StagedPt *pb, int eo,
-                                             float q, float floor_hat, float &chi_a, float &t_a,
-                                             float &chi_b, float &t_b) {
-    const float4 ra = *reinterpret_cast<const float4 *>(pa);
-    const float4 rb = *reinterpret_cast<const float4 *>(pb);
-    const float2 ea = reinterpret_cast<const float2 *>(pa)[eo];
-    const float2 eb = reinterpret_cast<const float2 *>(pb)[eo];
-    const unsigned long long d2 = pk2(ra.x, rb.x), q2 = pk2(q, q);
-    const unsigned long long off2 = fma2(d2, q2, add2(d2, q2));
-    const unsigned long long x2 = mul2(off2, pk2(ra.z, rb.z));
-    float xxa, xxb;
-    up2(mul2(x2, x2), xxa, xxb);
-    const unsigned long long g2 = pk2(ex2_approx(-xxa), ex2_approx(-xxb));
-    const unsigned long long rg2 = fma2(off2, g2, g2);
-    up2(fma2(pk2(ea.y, eb.y), rg2, pk2(floor_hat, floor_hat)), chi_a, chi_b);
-    up2(mul2(mul2(pk2(ea.x, eb.x), rg2), pk2(rcp_approx(chi_a), rcp_approx(chi_b))), t_a, t_b);
-    if (kCheck && chi_a < 0.5f * floor_hat) t_a = __int_as_float(0x7fc00000);
-    if (kCheck && chi_b < 0.5f * floor_hat) t_b = __int_as_float(0x7fc00000);
-}
-
 // Scaled Rybicki-Hummer state in projective form: F~ = a/b, S~ = c/b.  A
 // step then needs no division:
 //     Pb = P b,  a <- Q (Pb + a),  b <- Pb + 2a,  c <- Q (t Pb + c)
@@ -717,7 +666,8 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
     for (; s + 3 < e1; s += 4) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            staged_eval2<kCheck>(F + s + j, B + s + j, eo, q, floor_hat, chi, t_, chi2, t2);
+            staged_eval<kCheck>(F + s + j, eo, q, floor_hat, chi, t_);
+            staged_eval<kCheck>(B + s + j, eo, q, floor_hat, chi2, t2);
             fr.step(chi, t_, F[s + j].dzh);
             bk.step(chi2, t2, B[s + j].dzh);
         }
@@ -725,10 +675,12 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
         bk.renorm();
     }
     for (; s + 1 < e1; s += 2) {
-        staged_eval2<kCheck>(F + s, B + s, eo, q, floor_hat, chi, t_, chi2, t2);
+        staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
+        staged_eval<kCheck>(B + s, eo, q, floor_hat, chi2, t2);
         fr.step(chi, t_, F[s].dzh);
         bk.step(chi2, t2, B[s].dzh);
-        staged_eval2<kCheck>(F + s + 1, B + s + 1, eo, q, floor_hat, chi, t_, chi2, t2);
+        staged_eval<kCheck>(F + s + 1, eo, q, floor_hat, chi, t_);
+        staged_eval<kCheck>(B + s + 1, eo, q, floor_hat, chi2, t2);
         fr.step(chi, t_, F[s + 1].dzh);
         bk.step(chi2, t2, B[s + 1].dzh);
         fr.renorm();
@@ -743,20 +695,20 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
         bk.renorm();
         s++;
     }
-    // the rest of the front half: two consecutive points evaluated at once
+    // the rest of the front half
     for (; s + 3 < s1; s += 4) {
 #pragma unroll
-        for (int j = 0; j < 4; j += 2) {
-            staged_eval2<kCheck>(F + s + j, F + s + j + 1, eo, q, floor_hat, chi, t_, chi2, t2);
+        for (int j = 0; j < 4; j++) {
+            staged_eval<kCheck>(F + s + j, eo, q, floor_hat, chi, t_);
             fr.step(chi, t_, F[s + j].dzh);
-            fr.step(chi2, t2, F[s + j + 1].dzh);
         }
         fr.renorm();
     }
     for (; s + 1 < s1; s += 2) {
-        staged_eval2<kCheck>(F + s, F + s + 1, eo, q, floor_hat, chi, t_, chi2, t2);
+        staged_eval<kCheck>(F + s, eo, q, floor_hat, chi, t_);
         fr.step(chi, t_, F[s].dzh);
-        fr.step(chi2, t2, F[s + 1].dzh);
+        staged_eval<kCheck>(F + s + 1, eo, q, floor_hat, chi, t_);
+        fr.step(chi, t_, F[s + 1].dzh);
         fr.renorm();
     }
     if (s < s1) {
