@@ -75,6 +75,12 @@ struct mgr_handle {
     double *tshift = nullptr, *tdz = nullptr;
     MixedPoint *tmp_ = nullptr;        // mixed-format records
     int64_t tcap = 0;                  // point capacity of tcell/tshift/tdz
+    // far-end boundary intensities of the trace store for the staged mixed
+    // solve, [origins][npairs][2][nfreqs]; valid while bc_stamp == bc_serial
+    // (bc_serial counts changes of the traces, grid and boundary table)
+    float *bcache = nullptr;
+    int64_t bcache_cap = 0;            // origins
+    uint64_t bc_serial = 1, bc_stamp = 0;
     int32_t *blen = nullptr;           // batch lengths [nrays*bcap]
     int64_t *boff = nullptr;           // batch offsets
     int64_t bcap = 0;                  // origins per batch capacity
@@ -195,10 +201,13 @@ void free_traces(mgr_handle *h) {
     free_ptr((void *&)h->tmp_);
     free_ptr((void *&)h->blen);
     free_ptr((void *&)h->boff);
+    free_ptr((void *&)h->bcache);
     free_ptr(h->scan_tmp);
     h->scan_tmp_bytes = 0;
     h->tcap = 0;
     h->bcap = 0;
+    h->bcache_cap = 0;
+    h->bc_serial++;
     h->traced = false;
     h->stored = false;
     h->gen++;
@@ -599,11 +608,28 @@ void ensure_points(mgr_handle *h, int64_t npts) {
 
 constexpr int64_t kBytesPerPoint = sizeof(int32_t) + 2 * sizeof(double) + sizeof(MixedPoint);
 
-// 60% of the free device memory plus what the handle's point buffers hold.
+// Bytes per origin of the boundary cache (staged shapes only).
+int64_t bcache_bytes_per_origin(mgr_handle *h) {
+    return solve_is_staged(h->mv) ? (int64_t)h->npairs * 2 * h->nfreqs * (int64_t)sizeof(float) : 0;
+}
+
+// 60% of the free device memory plus what the handle's trace buffers hold.
 int64_t default_budget(mgr_handle *h) {
     size_t fr = 0, tot = 0;
     ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
-    return (int64_t)(0.6 * (double)fr) + h->tcap * kBytesPerPoint;
+    return (int64_t)(0.6 * (double)fr) + h->tcap * kBytesPerPoint +
+           h->bcache_cap * h->npairs * 2 * h->nfreqs * (int64_t)sizeof(float);
+}
+
+// Room for the boundary cache of `origins` origins (a new buffer changes the
+// captured graphs' arguments).
+void ensure_bcache(mgr_handle *h, int64_t origins) {
+    if (origins <= h->bcache_cap) return;
+    free_ptr((void *&)h->bcache);
+    h->bcache = dalloc<float>(h, origins * h->npairs * 2 * (int64_t)h->nfreqs, nullptr);
+    h->bcache_cap = origins;
+    h->bc_stamp = 0;
+    h->gen++;
 }
 
 // Host copy of the trace lengths (for get_npoints_on_rays and get_trace).
@@ -624,6 +650,7 @@ void do_trace(mgr_handle *h) {
     const void *old_bufs[] = {h->tcell, h->tshift, h->tdz, h->tmp_, h->off_all};
     const bool old_stored = h->stored;
     h->traced = false;
+    h->bc_serial++;
     h->stored = false;
     h->h_len_valid = false;
     const int old_max_pair = h->max_pair_points;
@@ -662,7 +689,8 @@ void do_trace(mgr_handle *h) {
     }
     h->total_points = total;
     const int64_t budget = h->trace_budget > 0 ? h->trace_budget : default_budget(h);
-    if (total * kBytesPerPoint <= budget) {
+    const int64_t per_origin_cache = bcache_bytes_per_origin(h);
+    if (total * kBytesPerPoint + N * per_origin_cache <= budget) {
         if (!h->off_all) h->off_all = dalloc<int64_t>(h, n, nullptr);
         const int64_t tot = scan_lengths(h, h->len_all, h->off_all, n);
         ensure_points(h, tot);
@@ -679,16 +707,16 @@ void do_trace(mgr_handle *h) {
         std::vector<int32_t> per_origin(N);
         ck(cudaMemcpy(per_origin.data(), h->pts_origin_d, N * sizeof(int32_t),
                       cudaMemcpyDeviceToHost), "d2h points");
-        const int64_t cap_pts = std::max<int64_t>(budget / kBytesPerPoint, 1);
         int64_t best = N;
         for (;;) {
             int64_t worst = 0;
             for (int64_t o0 = 0; o0 < N; o0 += best) {
+                const int64_t o1 = std::min(N, o0 + best);
                 int64_t s = 0;
-                for (int64_t o = o0; o < std::min(N, o0 + best); o++) s += per_origin[o];
-                worst = std::max(worst, s);
+                for (int64_t o = o0; o < o1; o++) s += per_origin[o];
+                worst = std::max(worst, s * kBytesPerPoint + (o1 - o0) * per_origin_cache);
             }
-            if (worst <= cap_pts || best == 1) break;
+            if (worst <= budget || best == 1) break;
             best = std::max<int64_t>(1, best / 2);
         }
         h->batch_origins = best;
@@ -730,6 +758,7 @@ void boundary_table(mgr_handle *h) {
     h->launches += 1;
     ck(cudaStreamSynchronize(h->stream), "boundary sync");
     h->bdy_set = true;
+    h->bc_serial++;
 }
 
 void do_solve(mgr_handle *h, int precision, bool use_graph);
@@ -751,7 +780,19 @@ SolveArgs solve_args(mgr_handle *h) {
     a.olist = nullptr;
     a.redo_flag = h->redo_flag;
     a.redo_list = h->redo_list;
+    a.bcache = h->bcache;
     return a;
+}
+
+// A mixed solve of a staged shape reads the boundary cache; enqueue_bcache
+// fills it for origins [s_begin, s_end) of trace store t (stream work only).
+bool bcache_needed(mgr_handle *h, int precision) {
+    return precision == MGR_MIXED && solve_is_staged(h->mv);
+}
+void enqueue_bcache(mgr_handle *h, const TraceView &t, int64_t s_begin, int64_t s_end) {
+    ck(launch_bdy_cache(h->mv, t, s_begin, s_end, h->bcache, h->flags, h->stream),
+       "boundary cache");
+    h->launches += 1;
 }
 
 void solve_prepare(mgr_handle *h, int precision) {
@@ -927,6 +968,18 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
     solve_prepare(h, precision);
     bool timing = false;
     const int variant = solve_variant(h, precision, &timing);
+    const bool cache = bcache_needed(h, precision);
+    if (h->stored && cache) {
+        ensure_bcache(h, h->N);
+        if (h->bc_stamp != h->bc_serial) {   // once per trace, grid and boundary table
+            reset_flags(h);
+            TraceView t{0, h->N, h->nrays, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
+            enqueue_bcache(h, t, h->o_begin, h->o_end);
+            ck(cudaStreamSynchronize(h->stream), "boundary cache");
+            check_flags(h, "boundary cache");
+            h->bc_stamp = h->bc_serial;
+        }
+    }
     if (h->stored) {
         // the events stay outside the graph (a captured record only orders work)
         ck(cudaEventRecord(h->ev0, h->stream), "event");
@@ -951,6 +1004,7 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
         return;
     }
     // traces in batches of origins, rebuilt for every solve
+    if (cache) ensure_bcache(h, h->batch_origins);
     const SolveArgs a = solve_args(h);
     reset_flags(h);
     unsigned long long patched = 0;
@@ -967,6 +1021,7 @@ void do_solve(mgr_handle *h, int precision, bool use_graph) {
         const int64_t cnt = std::min(h->batch_origins, h->o_end - o0);
         ck(cudaEventRecord(h->batch_ev[2 * bi], h->stream), "event");
         TraceView t = build_batch(h, o0, cnt);
+        if (cache) enqueue_bcache(h, t, 0, cnt);
         ck(cudaEventRecord(h->batch_ev[2 * bi + 1], h->stream), "event");
         SolveArgs ab = a;   // a batch's store holds exactly the origins it solves
         ab.s_begin = 0;
@@ -1250,6 +1305,7 @@ mgr_status mgr_compute_spectral_discretisation(mgr_handle *h) {
                              " (frequency grid not ascending); the device path needs separated lines");
             }
         h->line_set = true;
+        h->bc_serial++;
     });
 }
 

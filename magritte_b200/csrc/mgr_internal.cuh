@@ -305,6 +305,8 @@ struct SolveArgs {
     const int32_t *olist;           // when set: solve origins olist[s_begin .. s_end) instead
     int32_t *redo_flag;             // [N] mixed: 1 once an origin is listed for an FP64 re-solve
     int32_t *redo_list;             // [N] mixed: origins whose failures overflowed the patch list
+    const float *bcache;            // staged mixed solve: far-end boundary intensities of the
+                                    // trace store, [o_count][npairs][2][nfreqs] (launch_bdy_cache)
 };
 // Formal solve of the origins of one trace store.  variant selects the
 // register budget (one of kSolveVariants compiled resident-block counts;
@@ -314,6 +316,14 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
                                 int precision, int variant, DevFlags *flags, cudaStream_t s,
                                 int *kind);
 int solve_variant_blocks(int variant);
+// True when a solve of this model runs the staged kernels (no overlapping
+// lines, 31+ bins per line): the mixed one reads SolveArgs::bcache.
+bool solve_is_staged(const ModelView &m);
+// Fills cache[(oi * npairs + r) * 2 + h][f] for the origins [s_begin,
+// s_end) of trace store t: the boundary intensity at the far end of half h
+// (0: the longer one) of pair r, at bin f's frequency Doppler-shifted there.
+cudaError_t launch_bdy_cache(const ModelView &m, const TraceView &t, int64_t s_begin,
+                             int64_t s_end, float *cache, DevFlags *flags, cudaStream_t s);
 
 struct LevelArgs {
     double *pop, *prev1, *prev2, *prev3;   // [N*nlev]

@@ -631,22 +631,19 @@ constexpr int kStageSteps = MGR_STAGE_STEPS;
 
 // The sweep steps [s0, s1) of one staged window (front step s at F[s], back
 // step s at B[s]).
+// I0 and In are the boundary intensities at the two far ends.
 template <bool kCheck>
 __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt *B, int s0, int s1,
                                               int nbk, int eo, float q, float floor_hat,
-                                              const BdyCtx &bc, const BinCtx &b, DevFlags *flags,
-                                              ProjChain &fr, ProjChain &bk, double &I0,
-                                              double &In) {
+                                              ProjChain &fr, ProjChain &bk, double I0, double In) {
     float chi, t_, chi2, t2;
     int s = s0;
     if (s == 0) {
         staged_eval<kCheck>(F, eo, q, floor_hat, chi, t_);
         fr.start(chi, t_, F->dzh);
-        I0 = boundary_intensity(bc, (1.0 + (double)F->delta) * b.nu_o, F->cell, flags, b.k);
         if (nbk > 0) {
             staged_eval<kCheck>(B, eo, q, floor_hat, chi, t_);
             bk.start(chi, t_, B->dzh);
-            In = boundary_intensity(bc, (1.0 + (double)B->delta) * b.nu_o, B->cell, flags, b.k);
         }
         s = 1;
     }
@@ -723,19 +720,23 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
 // its point nfr-1-s (the far end first) and likewise for the back; each
 // lane eliminates both halves toward the origin, in lock step while both
 // have points.  A window with a line whose inverted opacity can take chi
-// below half the floor runs the checking variant of the sweep.
+// below half the floor runs the checking variant of the sweep.  bc_pair
+// holds the far ends' boundary intensities of this pair (front, then back;
+// nfreqs each), loaded before the first window is staged so that their
+// latency overlaps the staging.
 __device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, const float2 *ek,
                                             int K, int k0, int k1, int64_t ofr, int nfr,
                                             int64_t obk, int nbk, int eo, float q, float floor_hat,
-                                            const BdyCtx &bc, const BinCtx &b, float chi_o, float t_o,
-                                            const ModelView &m, int origin, int lane,
+                                            const float *bc_pair, const BinCtx &b, float chi_o,
+                                            float t_o, const ModelView &m, int origin, int lane,
                                             DevFlags *flags, double &u, double &L) {
     constexpr float kSqrtLog2e = 1.2011224087864498f;
     // an inverted line whose opacity can take chi below half the floor
     // (the profile factor (1 + off) exp(-x^2) stays below 1.001)
     const float neg_cut = -0.499f * floor_hat;
     ProjChain fr, bk;
-    double I0 = 0.0, In = 0.0;
+    double I0 = (double)__ldcs(bc_pair + b.f);
+    double In = nbk > 0 ? (double)__ldcs(bc_pair + m.nfreqs + b.f) : 0.0;
     for (int s0 = 0; s0 < nfr; s0 += kStageSteps) {
         const int s1 = min(s0 + kStageSteps, nfr);
         const int nF = s1 - s0;
@@ -759,9 +760,9 @@ __device__ __forceinline__ void staged_pair(StagedPt *buf, const TraceView &t, c
         const StagedPt *F = buf - s0;                 // front step s at F[s]
         const StagedPt *B = buf + kStageSteps - s0;   // back step s at B[s]
         if (check)
-            staged_window<true>(F, B, s0, s1, nbk, eo, q, floor_hat, bc, b, flags, fr, bk, I0, In);
+            staged_window<true>(F, B, s0, s1, nbk, eo, q, floor_hat, fr, bk, I0, In);
         else
-            staged_window<false>(F, B, s0, s1, nbk, eo, q, floor_hat, bc, b, flags, fr, bk, I0, In);
+            staged_window<false>(F, B, s0, s1, nbk, eo, q, floor_hat, fr, bk, I0, In);
         __syncwarp();
     }
     // the origin row
@@ -1032,8 +1033,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
                 staged_pair64(pts, t, a.eps, a.kap, K, k0, k1, ofr, nfr, obk, nbk, ln, bc, b, c64,
                               t_o64, m, o, lane, flags, u, L);
             } else {
-                staged_pair(pts, t, ek, K, k0, k1, ofr, nfr, obk, nbk, eo, b.q, floor_hat, bc, b,
-                            chi_o, t_o, m, o, lane, flags, u, L);
+                staged_pair(pts, t, ek, K, k0, k1, ofr, nfr, obk, nbk, eo, b.q, floor_hat,
+                            a.bcache + ((oi * m.npairs + r) * 2) * (int64_t)nf, b, chi_o, t_o, m,
+                            o, lane, flags, u, L);
             }
             if (!kFp64 && !(isfinite(u) && isfinite(L))) {
                 const unsigned long long slot = atomicAdd(a.patch_count, 1ull);
@@ -1066,7 +1068,67 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     }
 }
 
+// One warp per (origin, pair) of a trace store, lanes over bins: the far
+// ends' boundary intensities that the staged mixed solve reads
+// (Radiation::rescale_I_bdy at the Doppler-shifted frequency, as the other
+// kernels evaluate it inline, from the same far-end records and the same
+// origin frequencies).  They depend only on the traces, the frequency grid
+// and the boundary table, so one fill serves every solve over a store.
+__global__ void __launch_bounds__(256)
+    bdy_cache_kernel(ModelView m, TraceView t, int64_t s_begin, int64_t s_end, float *cache,
+                     DevFlags *flags) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t ntask = (s_end - s_begin) * m.npairs;
+    const BdyCtx bc = bdy_ctx(m);
+    const int nq = m.nquads, nf = m.nfreqs;
+    for (int64_t task = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+         task < ntask; task += nwarps) {
+        const int64_t oi = s_begin + task / m.npairs;
+        const int r = (int)(task % m.npairs);
+        const int o = (int)(t.o_begin + oi);
+        const int ar = m.antipod[r];
+        const int64_t ir = (int64_t)r * t.o_count + oi;
+        const int64_t iar = (int64_t)ar * t.o_count + oi;
+        const int nr_ = t.len[ir], nar_ = t.len[iar];
+        const bool rfront = nr_ > nar_;
+        const int nfr = rfront ? nr_ : nar_;
+        const int nbk = rfront ? nar_ : nr_;
+        if (nfr == 0) continue;   // the solve takes this origin's own boundary value
+        const int64_t ofr = rfront ? t.off[ir] : t.off[iar];
+        const int64_t obk = rfront ? t.off[iar] : t.off[ir];
+        // far-end records: x = cell (bits), y = Doppler shift - 1
+        const float4 vf = __ldg(reinterpret_cast<const float4 *>(t.mp) + ofr + nfr - 1);
+        const float4 vb = nbk > 0 ? __ldg(reinterpret_cast<const float4 *>(t.mp) + obk + nbk - 1)
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+        const double pw_o = m.pw[o];
+        float *row = cache + (oi * m.npairs + r) * 2 * (int64_t)nf;
+        for (int f = lane; f < nf; f += 32) {
+            const int k = f / nq, z = f - k * nq;
+            const double line_k = m.line[k];
+            const double nu_o = radd(line_k, rmul(rmul(line_k, pw_o), m.roots[z]));
+            row[f] = (float)boundary_intensity(bc, (1.0 + (double)vf.y) * nu_o,
+                                               __float_as_int(vf.x), flags, k);
+            if (nbk > 0)
+                row[nf + f] = (float)boundary_intensity(bc, (1.0 + (double)vb.y) * nu_o,
+                                                        __float_as_int(vb.x), flags, k);
+        }
+    }
+}
+
 }  // namespace
+
+bool solve_is_staged(const ModelView &m) { return !m.overlap && m.nquads >= 31; }
+
+cudaError_t launch_bdy_cache(const ModelView &m, const TraceView &t, int64_t s_begin,
+                             int64_t s_end, float *cache, DevFlags *flags, cudaStream_t s) {
+    if (s_end <= s_begin) return cudaSuccess;
+    if (!cache) return cudaErrorInvalidValue;
+    const int64_t warps = (s_end - s_begin) * m.npairs;
+    const unsigned blocks = (unsigned)std::min<int64_t>((warps + 7) / 8, 148 * 32);
+    bdy_cache_kernel<<<blocks, 256, 0, s>>>(m, t, s_begin, s_end, cache, flags);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const SolveArgs &a,
                                 int precision, int variant, DevFlags *flags, cudaStream_t s,
@@ -1076,7 +1138,8 @@ cudaError_t launch_formal_solve(const ModelView &m, const TraceView &t, const So
     const size_t shmem = (size_t)kWarpsPerBlock * 2 * m.nrad * sizeof(double);
     // the staged kernels need each 32-bin chunk within two lines and lines
     // whose windows do not overlap
-    const bool staged = !m.overlap && m.nquads >= 31;
+    const bool staged = solve_is_staged(m);
+    if (staged && precision == MGR_MIXED && !a.bcache) return cudaErrorInvalidValue;
     if (kind) *kind = staged ? 1 : 0;
     if (variant < 0 || variant >= kSolveVariants)
         variant = !staged ? kDefaultGeneric : precision == MGR_FP64 ? kDefaultStaged64 : kDefaultStaged;
