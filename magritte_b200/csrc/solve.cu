@@ -1068,24 +1068,103 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks)
     }
 }
 
+// The far end of one half for the boundary cache: its boundary row and
+// its profile width, resolved once per (origin, pair).
+struct FarEnd {
+    const double *I;   // I_bdy on the far cell's grid, or null (not a boundary cell)
+    double pwp, ipwp;
+    double shift;      // 1 + Doppler shift - 1 of the far end
+};
+
+__device__ __forceinline__ FarEnd far_end(const BdyCtx &c, float4 rec, DevFlags *flags) {
+    FarEnd e;
+    const int p = __float_as_int(rec.x);
+    const int b = __ldg(c.cell2bdy + p);
+    e.I = nullptr;
+    if (b >= 0) e.I = c.ibdy + (int64_t)b * c.nf;
+    else atomicAdd(&flags->trace_err, 1ull);
+    e.pwp = __ldg(c.pw + p);
+    e.ipwp = __ldg(c.inv_pw + p);
+    e.shift = 1.0 + (double)rec.y;
+    return e;
+}
+
+// boundary_intensity's bin search on the far cell's grid, with the
+// interpolation weight formed in double and applied with one float
+// division (the cache holds floats).  The line is searched from the lane's
+// own line k: a Doppler shift of many profile widths moves the frequency
+// out of line k's window, but on a grid of separated lines only to the gap
+// below line k (line k or k - 1 then holds the first bin at or above it)
+// or the gap above (line k + 1); a bisection covers the rest.  The bin is
+// then found from the root-grid guess and walked.
+__device__ __forceinline__ float far_end_intensity(const BdyCtx &c, const FarEnd &e, double freq,
+                                                   int k) {
+    const int nq = c.nq, nf = c.nf, K = nf / nq;
+    if (!e.I) return 0.0f;
+    auto nu_kz = [&](int kk, int z) {
+        const double line = __ldg(c.line + kk);
+        return radd(line, rmul(rmul(line, e.pwp), __ldg(c.roots + z)));
+    };
+    // the first line whose last bin is >= freq, within [lo, hi)
+    auto bisect = [&](int lo, int hi) {
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (freq <= nu_kz(mid, nq - 1)) hi = mid;
+            else lo = mid + 1;
+        }
+        return lo;
+    };
+    int lo;
+    if (freq <= nu_kz(k, nq - 1)) {
+        if (k == 0 || freq > nu_kz(k - 1, nq - 1)) lo = k;
+        else if (k == 1 || freq > nu_kz(k - 2, nq - 1)) lo = k - 1;
+        else lo = bisect(0, k - 1);
+    } else {
+        if (k + 1 < K && freq <= nu_kz(k + 1, nq - 1)) lo = k + 1;
+        else lo = bisect(k + 1, K);
+        if (lo == K) return (float)__ldg(e.I + nf - 1);   // above the grid
+    }
+    const double root = (freq * __ldg(c.inv_line + lo) - 1.0) * e.ipwp;
+    const double zg = ceil((root - __ldg(c.roots)) * c.root_inv_step);
+    int zl = (int)fmin(fmax(zg, 0.0), (double)(nq - 1));
+    double nu1 = nu_kz(lo, zl);
+    while (zl < nq - 1 && freq > nu1) nu1 = nu_kz(lo, ++zl);
+    double nu2 = zl > 0 ? nu_kz(lo, zl - 1) : (lo > 0 ? nu_kz(lo - 1, nq - 1) : 0.0);
+    while (zl > 0 && freq <= nu2) {
+        nu1 = nu2;
+        zl--;
+        nu2 = zl > 0 ? nu_kz(lo, zl - 1) : (lo > 0 ? nu_kz(lo - 1, nq - 1) : 0.0);
+    }
+    const int notch = lo * nq + zl;
+    const double I1 = __ldg(e.I + notch);
+    if (notch == 0 || notch == nf - 1) return (float)I1;
+    const double I2 = __ldg(e.I + notch - 1);
+    const float w = __fdividef((float)(freq - nu1), (float)(nu2 - nu1));
+    return (float)fma((double)w, I2 - I1, I1);
+}
+
 // One warp per (origin, pair) of a trace store, lanes over bins: the far
 // ends' boundary intensities that the staged mixed solve reads
-// (Radiation::rescale_I_bdy at the Doppler-shifted frequency, as the other
-// kernels evaluate it inline, from the same far-end records and the same
-// origin frequencies).  They depend only on the traces, the frequency grid
-// and the boundary table, so one fill serves every solve over a store.
+// (Radiation::rescale_I_bdy at the Doppler-shifted frequency, from the same
+// far-end records and origin frequencies as the solve).  They depend only
+// on the traces, the frequency grid and the boundary table, so one fill
+// serves every solve over a store.
 __global__ void __launch_bounds__(256)
     bdy_cache_kernel(ModelView m, TraceView t, int64_t s_begin, int64_t s_end, float *cache,
                      DevFlags *flags) {
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    const int64_t ntask = (s_end - s_begin) * m.npairs;
+    const int np = m.npairs;
+    const int64_t ntask = (s_end - s_begin) * np;
     const BdyCtx bc = bdy_ctx(m);
     const int nq = m.nquads, nf = m.nfreqs;
+    // this lane's first bin: line k0, root z0; each further chunk moves
+    // 32 bins on (32 - nq wraps to the next line at most twice for nq >= 11)
+    const int k0 = lane / nq, z0 = lane - k0 * nq;
     for (int64_t task = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
          task < ntask; task += nwarps) {
-        const int64_t oi = s_begin + task / m.npairs;
-        const int r = (int)(task % m.npairs);
+        const int64_t oi = s_begin + task / np;
+        const int r = (int)(task - (oi - s_begin) * np);
         const int o = (int)(t.o_begin + oi);
         const int ar = m.antipod[r];
         const int64_t ir = (int64_t)r * t.o_count + oi;
@@ -1098,20 +1177,21 @@ __global__ void __launch_bounds__(256)
         const int64_t ofr = rfront ? t.off[ir] : t.off[iar];
         const int64_t obk = rfront ? t.off[iar] : t.off[ir];
         // far-end records: x = cell (bits), y = Doppler shift - 1
-        const float4 vf = __ldg(reinterpret_cast<const float4 *>(t.mp) + ofr + nfr - 1);
-        const float4 vb = nbk > 0 ? __ldg(reinterpret_cast<const float4 *>(t.mp) + obk + nbk - 1)
-                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+        const FarEnd ef = far_end(bc, __ldg(reinterpret_cast<const float4 *>(t.mp) + ofr + nfr - 1),
+                                  flags);
+        FarEnd eb{nullptr, 0.0, 0.0, 1.0};
+        if (nbk > 0)
+            eb = far_end(bc, __ldg(reinterpret_cast<const float4 *>(t.mp) + obk + nbk - 1), flags);
         const double pw_o = m.pw[o];
-        float *row = cache + (oi * m.npairs + r) * 2 * (int64_t)nf;
+        float *row = cache + (oi * np + r) * 2 * (int64_t)nf;
+        int k = k0, z = z0;
         for (int f = lane; f < nf; f += 32) {
-            const int k = f / nq, z = f - k * nq;
-            const double line_k = m.line[k];
-            const double nu_o = radd(line_k, rmul(rmul(line_k, pw_o), m.roots[z]));
-            row[f] = (float)boundary_intensity(bc, (1.0 + (double)vf.y) * nu_o,
-                                               __float_as_int(vf.x), flags, k);
-            if (nbk > 0)
-                row[nf + f] = (float)boundary_intensity(bc, (1.0 + (double)vb.y) * nu_o,
-                                                        __float_as_int(vb.x), flags, k);
+            const double line_k = __ldg(m.line + k);
+            const double nu_o = radd(line_k, rmul(rmul(line_k, pw_o), __ldg(m.roots + z)));
+            __stcs(row + f, far_end_intensity(bc, ef, ef.shift * nu_o, k));
+            if (nbk > 0) __stcs(row + nf + f, far_end_intensity(bc, eb, eb.shift * nu_o, k));
+            z += 32;
+            while (z >= nq) { z -= nq; k++; }
         }
     }
 }
