@@ -130,7 +130,9 @@ const char *mgr_version(void);
  * boundary maps.  Replaces Simulation::read (Model/model.cpp). */
 mgr_status mgr_upload_model(mgr_handle *h, const mgr_model_desc *model);
 
-/* Caps device memory used for stored ray traces (bytes; 0 = automatic).
+/* Caps device memory used for stored ray traces (bytes; 0 = automatic):
+ * the traced points and, for models the staged kernels solve, the far-end
+ * boundary cache of the mixed solve (8 B per ray pair and bin per origin).
  * Beyond it, traces are recomputed per batch of origins each solve. */
 mgr_status mgr_set_trace_budget(mgr_handle *h, int64_t bytes);
 
