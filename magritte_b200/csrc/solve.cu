@@ -580,11 +580,14 @@ __device__ __forceinline__ void staged_eval(const StagedPt *p, int eo, float q, 
 
 // Scaled Rybicki-Hummer state in projective form: F~ = a/b, S~ = c/b.  A
 // step then needs no division:
-//     Pb = P b,  a <- Q (Pb + a),  b <- Pb + 2a,  c <- Q (t Pb + c)
-// (from F~ <- w/(P + 2w), w = Q (P + F~), and S~ <- (t P + S~) Q/(P + 2w),
-// multiplied through by b).  Every term is non-negative for non-negative
-// opacities, so nothing cancels; a, b, c are rescaled by a power of two
-// every second step, which keeps them in range for any optical depth.
+//     X = dh' b,  Pb = H X,  a <- dh (Pb + a),  b <- X + 2a,  c <- dh (t Pb + c)
+// with dh' the previous half optical depth and H = dh' + dh (from
+// F~ <- w/(P + 2w), w = Q (P + F~), and S~ <- (t P + S~) Q/(P + 2w), where
+// P = H dh' and Q = H dh, multiplied through by b/H).  Every term is
+// non-negative for non-negative opacities, so nothing cancels; per step b
+// shrinks by at most dh' and grows by at most about 4 dh^3, and a, b, c are
+// rescaled by a power of two every few steps, which keeps them in range for
+// any optical depth.
 // R is the type of the staged point values (float in mixed precision,
 // double in FP64); the elimination itself is always double.
 template <class R>
@@ -608,11 +611,11 @@ struct ProjChainT {
     __device__ __forceinline__ void step(R chi_b, R t_b, R dzh_b) {
         const double dh = (double)((chi_a + chi_b) * dzh_a);
         const double H = dh_prev + dh;
-        const double P = H * dh_prev, Q = H * dh;
-        const double Pb = P * b;
-        a = Q * (Pb + a);
-        c = Q * fma((double)t_a, Pb, c);
-        b = fma(2.0, a, Pb);
+        const double X = dh_prev * b;
+        const double Pb = H * X;
+        a = dh * (Pb + a);
+        c = dh * fma((double)t_a, Pb, c);
+        b = fma(2.0, a, X);
         dh_prev = dh;
         chi_a = chi_b; t_a = t_b; dzh_a = dzh_b;
     }
@@ -656,9 +659,10 @@ __device__ __forceinline__ void staged_window(const StagedPt *F, const StagedPt 
         }
         s = 2;
     }
-    // both halves: four steps between renormalisations (b shrinks by at
-    // most dh^2 per step, dh >= ~5e-20 on floor-opacity sub-points, so four
-    // steps stay far inside the double range)
+    // both halves: four steps between renormalisations (per step b shrinks
+    // by at most dh >= ~5e-20, on floor-opacity sub-points, and grows by at
+    // most ~4 dh^3, so four steps stay inside the double range for half
+    // optical depths up to ~1e19)
     const int e1 = min(s1, nbk);
     for (; s + 3 < e1; s += 4) {
 #pragma unroll
