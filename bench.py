@@ -51,11 +51,11 @@ METRIC = "ALI iters & wall-clock to 1e-4 pops on 1 B200: learned+FP32 vs plain F
 TOL = 1.0e-4
 MAX_ITER = 400
 FALLBACK_HBM_GBS = 6650.0
-STAGED_DRAM_BYTES_PER_UPDATE = 0.686
+STAGED_DRAM_BYTES_PER_UPDATE = 0.685
 # thread instructions (warp instructions x 32) per update of the same kernel
 # in the same capture: the issue-bound ceiling is 148 SMs x 4 schedulers x
 # the SM clock x 32 lanes / this
-STAGED_THREAD_INST_PER_UPDATE = 35.2
+STAGED_THREAD_INST_PER_UPDATE = 34.2
 B200_SMS = 148
 
 
