@@ -81,6 +81,11 @@ struct mgr_handle {
     float *bcache = nullptr;
     int64_t bcache_cap = 0;            // origins
     uint64_t bc_serial = 1, bc_stamp = 0;
+    // hop log of the counting pass (HopLog): the fill of a stored trace
+    // replays it instead of searching; [kHopCap][nrays*N] cells and
+    // [nrays*N] counts
+    int32_t *hop_cell = nullptr, *hop_n = nullptr;
+    int64_t hop_rays = 0;
     int32_t *blen = nullptr;           // batch lengths [nrays*bcap]
     int64_t *boff = nullptr;           // batch offsets
     int64_t bcap = 0;                  // origins per batch capacity
@@ -202,6 +207,9 @@ void free_traces(mgr_handle *h) {
     free_ptr((void *&)h->blen);
     free_ptr((void *&)h->boff);
     free_ptr((void *&)h->bcache);
+    free_ptr((void *&)h->hop_cell);
+    free_ptr((void *&)h->hop_n);
+    h->hop_rays = 0;
     free_ptr(h->scan_tmp);
     h->scan_tmp_bytes = 0;
     h->tcap = 0;
@@ -607,6 +615,8 @@ void ensure_points(mgr_handle *h, int64_t npts) {
 }
 
 constexpr int64_t kBytesPerPoint = sizeof(int32_t) + 2 * sizeof(double) + sizeof(MixedPoint);
+// Hops of a walk the counting pass logs (longer walks are searched again).
+constexpr int64_t kHopCap = 128;
 
 // Bytes per origin of the boundary cache (staged shapes only).
 int64_t bcache_bytes_per_origin(mgr_handle *h) {
@@ -662,8 +672,29 @@ void do_trace(mgr_handle *h) {
         if (!h->h_tstats) ck(cudaMallocHost(&h->h_tstats, 3 * sizeof(unsigned long long)), "pinned");
     }
     if (h->nseg > 0 && !h->upd_origin_d) h->upd_origin_d = dalloc<float>(h, N, nullptr);
+    // log the walks' hops when the log takes at most a tenth of the free
+    // memory (and the caller set no trace budget): the fill then replays them
+    bool logged = false;
+    if (h->trace_budget == 0) {
+        const int64_t bytes = n * (kHopCap + 1) * (int64_t)sizeof(int32_t);
+        size_t fr = 0, tot = 0;
+        ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+        const int64_t held = h->hop_rays * (kHopCap + 1) * (int64_t)sizeof(int32_t);
+        if (bytes <= ((int64_t)fr + held) / 10) {
+            if (h->hop_rays != n) {
+                free_ptr((void *&)h->hop_cell);
+                free_ptr((void *&)h->hop_n);
+                h->hop_cell = dalloc<int32_t>(h, n * kHopCap, nullptr);
+                h->hop_n = dalloc<int32_t>(h, n, nullptr);
+                h->hop_rays = n;
+            }
+            logged = true;
+        }
+    }
+    const HopLog hop_log{h->hop_cell, h->hop_n, (int)kHopCap};
     reset_flags(h);
-    ck(launch_trace_count(h->mv, 0, N, h->len_all, h->flags, h->stream), "trace count");
+    ck(launch_trace_count(h->mv, 0, N, h->len_all, h->flags, h->stream, logged ? &hop_log : nullptr),
+       "trace count");
     // ray-point-frequency updates of one formal solve, the longest pair and
     // the points per origin, reduced on the device
     ck(launch_trace_stats(h->mv, h->len_all, h->tstats_d, h->pts_origin_d,
@@ -696,7 +727,8 @@ void do_trace(mgr_handle *h) {
         ensure_points(h, tot);
         TraceView t{0, N, (int)R, h->off_all, h->len_all, h->tcell, h->tshift, h->tdz, h->tmp_};
         reset_flags(h);
-        ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->tmp_, h->flags, h->stream),
+        ck(launch_trace_fill(h->mv, t, h->tcell, h->tshift, h->tdz, h->tmp_, h->flags, h->stream,
+                             logged ? &hop_log : nullptr),
            "trace fill");
         h->launches += 1;
         check_flags(h, "trace fill");

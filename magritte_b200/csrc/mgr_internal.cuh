@@ -235,11 +235,23 @@ static __device__ __forceinline__ double boundary_intensity(BdyCtx c, double fre
 
 // ------------------------------------------------------------------------
 // Host-side launchers (each file owns its kernels).
+// The neighbour each hop of a walk chose, recorded by the counting pass
+// so that the filling pass replays the walk without searching: cell[k *
+// nrays_total + idx] for hops k < cap of ray idx, and n[idx] = the ray's hop
+// count, or -1 when it has more than cap hops (the fill then searches).
+struct HopLog {
+    int32_t *cell;
+    int32_t *n;
+    int cap;
+};
 cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_count,
-                               int32_t *len, DevFlags *flags, cudaStream_t s);
+                               int32_t *len, DevFlags *flags, cudaStream_t s,
+                               const HopLog *hops = nullptr);
+// hops: the log of the counting pass over the same rays (o_begin = 0,
+// o_count = N), or null to search every walk again.
 cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
                               double *shift, double *dZ, MixedPoint *mp, DevFlags *flags,
-                              cudaStream_t s);
+                              cudaStream_t s, const HopLog *hops = nullptr);
 // Rest-frame traces of the two rays of an image for every origin: slot
 // d * N + o walks ray_front (d = 0) or ray_back (d = 1), its shift projected
 // on ray shift_front or shift_back.

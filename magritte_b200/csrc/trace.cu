@@ -75,6 +75,17 @@ struct Walker {
         Z = radd(Z, dZ);
         return nxt;
     }
+
+    // The same step along a known next cell nb (the one next() chose): its
+    // projection and increment by the same operations.
+    __device__ __forceinline__ double advance(int64_t nb, double &Z) const {
+        const double Rx = rsub(__ldg(m.pos + 3 * nb + 0), ox);
+        const double Ry = rsub(__ldg(m.pos + 3 * nb + 1), oy);
+        const double Rz = rsub(__ldg(m.pos + 3 * nb + 2), oz);
+        const double dZ = rsub(rdot3(Rx, Ry, Rz, rx, ry, rz), Z);
+        Z = radd(Z, dZ);
+        return dZ;
+    }
 };
 
 // Sink that only counts points.
@@ -142,13 +153,27 @@ __device__ __forceinline__ bool set_data(int64_t crt, int64_t nxt, double shift_
 // Geometry::trace_ray<CoMoving> (geometry.tpp:21-95).  Returns 0 or an
 // error code: 1 no neighbour ahead, 2 too many interpolation points,
 // 3 step limit.
+// With a hop log (log, stride = the rays of the log, idx = this ray), each
+// hop's cell is recorded while it fits the log's capacity, and the hop
+// count (or -1 beyond it) at the end of a walk without error.
 template <class Sink>
-__device__ int walk(const ModelView &m, int64_t o, int d, Sink &sink, int shift_dir = -1) {
+__device__ int walk(const ModelView &m, int64_t o, int d, Sink &sink, int shift_dir = -1,
+                    const HopLog *log = nullptr, int64_t stride = 0, int64_t idx = 0) {
     const Walker w(m, o, d, shift_dir);
     const double dsm = m.dshift_max[o];
     double Z = 0.0, dZ = 0.0;
+    int hops = 0;
+    auto record = [&](int64_t c) {
+        if (log && hops < log->cap) log->cell[(int64_t)hops * stride + idx] = (int32_t)c;
+        hops++;
+    };
+    auto finish = [&]() {
+        if (log) log->n[idx] = hops <= log->cap ? hops : -1;
+        return 0;
+    };
     int64_t nxt = w.next(o, Z, dZ);
-    if (nxt == -1) return 0;
+    if (nxt == -1) return finish();
+    record(nxt);
     int64_t crt = o;
     double shift_crt = w.shift(crt);
     double shift_nxt = w.shift(nxt);
@@ -160,8 +185,31 @@ __device__ int walk(const ModelView &m, int64_t o, int d, Sink &sink, int shift_
         crt = nxt;
         nxt = w.next(nxt, Z, dZ);
         if (nxt < 0) return 1;
+        record(nxt);
         shift_nxt = w.shift(nxt);
         if (!set_data(crt, nxt, shift_crt, shift_nxt, dZ, dsm, sink)) return 2;
+    }
+    return finish();
+}
+
+// The walk of a ray whose hops the counting pass logged: the same points
+// from the logged cells, without the neighbour search.  Returns 0, or 2 if
+// set_data fails (it cannot where the counting pass succeeded).
+template <class Sink>
+__device__ int replay(const ModelView &m, int64_t o, int d, const HopLog &log, int64_t stride,
+                      int64_t idx, int nh, Sink &sink) {
+    const Walker w(m, o, d, -1);
+    const double dsm = m.dshift_max[o];
+    double Z = 0.0;
+    int64_t crt = o;
+    double shift_crt = w.shift(crt);
+    for (int k = 0; k < nh; k++) {
+        const int64_t nxt = __ldg(log.cell + (int64_t)k * stride + idx);
+        const double dZ = w.advance(nxt, Z);
+        const double shift_nxt = w.shift(nxt);
+        if (!set_data(crt, nxt, shift_crt, shift_nxt, dZ, dsm, sink)) return 2;
+        crt = nxt;
+        shift_crt = shift_nxt;
     }
     return 0;
 }
@@ -174,14 +222,15 @@ __device__ __forceinline__ void count_error(DevFlags *f, int code) {
 
 __global__ void __launch_bounds__(128) trace_count_kernel(ModelView m, int64_t o_begin,
                                                           int64_t o_count, int32_t *len,
-                                                          DevFlags *flags) {
+                                                          DevFlags *flags, HopLog log,
+                                                          bool logged) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t total = (int64_t)m.nrays * o_count;
     if (idx >= total) return;
     const int d = (int)(idx / o_count);
     const int64_t o = o_begin + idx % o_count;
     CountSink sink;
-    const int code = walk(m, o, d, sink);
+    const int code = walk(m, o, d, sink, -1, logged ? &log : nullptr, total, idx);
     if (code) count_error(flags, code);
     len[idx] = code ? 0 : (int32_t)sink.n;
 }
@@ -189,7 +238,8 @@ __global__ void __launch_bounds__(128) trace_count_kernel(ModelView m, int64_t o
 __global__ void __launch_bounds__(128) trace_fill_kernel(ModelView m, TraceView t,
                                                          int32_t *cell, double *shift,
                                                          double *dZ, MixedPoint *mp,
-                                                         DevFlags *flags) {
+                                                         DevFlags *flags, HopLog log,
+                                                         bool logged) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t total = (int64_t)t.ndir * t.o_count;
     if (idx >= total) return;
@@ -204,7 +254,8 @@ __global__ void __launch_bounds__(128) trace_fill_kernel(ModelView m, TraceView 
     sink.mp = mp;
     sink.inv_pw = m.inv_pw;
     sink.half_inv_scale = 0.5 / m.mixed_scale;
-    const int code = walk(m, o, d, sink);
+    const int nh = logged ? log.n[idx] : -1;
+    const int code = nh >= 0 ? replay(m, o, d, log, total, idx, nh, sink) : walk(m, o, d, sink);
     if (code) count_error(flags, code);
     if (sink.over || (code == 0 && sink.n != sink.cap)) atomicAdd(&flags->cap_err, 1ull);
 }
@@ -321,23 +372,28 @@ cudaError_t launch_image_trace_fill(const ModelView &m, int ray_front, int ray_b
 }
 
 cudaError_t launch_trace_count(const ModelView &m, int64_t o_begin, int64_t o_count,
-                               int32_t *len, DevFlags *flags, cudaStream_t s) {
+                               int32_t *len, DevFlags *flags, cudaStream_t s,
+                               const HopLog *hops) {
     const int64_t total = (int64_t)m.nrays * o_count;
     if (total == 0) return cudaSuccess;
     const int threads = 128;
     const int64_t blocks = (total + threads - 1) / threads;
-    trace_count_kernel<<<(unsigned)blocks, threads, 0, s>>>(m, o_begin, o_count, len, flags);
+    trace_count_kernel<<<(unsigned)blocks, threads, 0, s>>>(
+        m, o_begin, o_count, len, flags, hops ? *hops : HopLog{nullptr, nullptr, 0}, hops != nullptr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_trace_fill(const ModelView &m, const TraceView &t, int32_t *cell,
                               double *shift, double *dZ, MixedPoint *mp, DevFlags *flags,
-                              cudaStream_t s) {
+                              cudaStream_t s, const HopLog *hops) {
     const int64_t total = (int64_t)t.ndir * t.o_count;
     if (total == 0) return cudaSuccess;
+    // a log indexes the rays of all origins: usable for a store of all of them
+    if (hops && (t.o_begin != 0 || t.o_count != m.N)) return cudaErrorInvalidValue;
     const int threads = 128;
     const int64_t blocks = (total + threads - 1) / threads;
-    trace_fill_kernel<<<(unsigned)blocks, threads, 0, s>>>(m, t, cell, shift, dZ, mp, flags);
+    trace_fill_kernel<<<(unsigned)blocks, threads, 0, s>>>(
+        m, t, cell, shift, dZ, mp, flags, hops ? *hops : HopLog{nullptr, nullptr, 0}, hops != nullptr);
     return cudaGetLastError();
 }
 
