@@ -7,7 +7,7 @@
 // so a zero network reproduces the LTE start of
 // LineProducingSpecies::update_using_LTE (lineProducingSpecies.tpp:82-115),
 // which stays the fallback.  The ALI iteration then runs to the same
-// tolerance from this start, so it also judges the network's error.
+// tolerance from this start, so it also checks the network's error.
 //
 // Everything here is hand-written SIMT FP32: the network is tiny
 // (10 -> 128 -> 128 -> 128 -> nlev, 35k parameters) and runs once per solve;

@@ -5,7 +5,7 @@ width, velocity-gradient length, column densities along the traced rays) to a
 correction of the LTE log level fractions; the populations
 n = n_tot softmax(log x_LTE + MLP(f)) replace the LTE start, and the plain
 ALI + Ng iteration then runs to the same tolerance, so it is both the
-fallback and the judge of the network's error.  The network is trained on
+fallback and the check on the network's error.  The network is trained on
 converged populations produced by this solver, with the library's own
 forward, backward and Adam kernels (``mgr_mlp_train``).
 
