@@ -17,9 +17,11 @@ solve from LTE is measured in the same run and reported beside it.
     roofline  the formal-solve kernel: algorithmic bytes (44 B per
            ray-point-frequency update in FP64, 24 B in mixed) / its average
            launch time, against the measured HBM copy bandwidth
-    cpu_baseline  the CPU oracle on this host's cores: one formal solve on a
-           sample of origins, extrapolated, plus the full rate-equation step,
-           times the iteration count of the solve
+    cpu_baseline  the reference's compiled CPU path (oracle/_ref; the C
+           oracle where that binary is absent) on this host's cores: the
+           per-origin work of one formal solve on a sample of origins,
+           extrapolated, plus the full rate-equation step, times the
+           iteration count of the solve
 
 ``--impl reference`` times the reference's own C++ (Magritte's CPU path
 compiled from its sources into oracle/_ref; the CPU oracle, the same
