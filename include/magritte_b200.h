@@ -97,7 +97,9 @@ typedef struct {
 /* Options of the ALI loop.  Replaces the arguments of
  * Simulation::compute_level_populations(io, use_Ng, max_niterations). */
 typedef struct {
-    int32_t use_ng;        /* Ng acceleration every 5th iteration          */
+    int32_t use_ng;        /* Ng acceleration after every ng_every normal
+                              iterations (the reference: every 5th
+                              iteration, i.e. after 4)                     */
     int32_t precision;     /* mgr_precision                                */
     int64_t max_iter;      /* 1000 in the reference's default overload     */
     double  tol_max_rel;   /* > 0: stop once max over (cell, level) of
@@ -105,7 +107,9 @@ typedef struct {
                               n > 1e-10 n_tot); <= 0: the reference's stop
                               test, fraction_not_converged <= 0.005        */
     int32_t use_graph;     /* replay each iteration as a CUDA graph        */
-    int32_t reserved;
+    int32_t ng_every;      /* normal iterations before each Ng step: 0 for
+                              the reference's 4, else >= 3 (the step reads
+                              the populations and three previous iterates) */
 } mgr_ali_opts;
 
 typedef struct mgr_handle mgr_handle;

@@ -88,7 +88,7 @@ class TrainOpts(C.Structure):
 
 class AliOpts(C.Structure):
     _fields_ = [("use_ng", _i32), ("precision", _i32), ("max_iter", _i64),
-                ("tol_max_rel", _dbl), ("use_graph", _i32), ("reserved", _i32)]
+                ("tol_max_rel", _dbl), ("use_graph", _i32), ("ng_every", _i32)]
 
 
 class Tuning(C.Structure):

@@ -1522,6 +1522,9 @@ mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts
     const mgr_status s = run(h, [&] {
         need(opts != nullptr, MGR_ERR_INVALID_ARG, "NULL options");
         need(opts->max_iter >= 1, MGR_ERR_INVALID_ARG, "max_iter must be >= 1");
+        need(opts->ng_every == 0 || opts->ng_every >= 3, MGR_ERR_INVALID_ARG,
+             "ng_every must be 0 (the reference's 4) or >= 3");
+        const int64_t ng_every = opts->ng_every > 0 ? opts->ng_every : 4;
         need(h->line_set, MGR_ERR_STATE, "compute_spectral_discretisation first");
         need(h->pops_valid, MGR_ERR_STATE, "no level populations yet");
         need(h->whole(), MGR_ERR_STATE,
@@ -1540,7 +1543,7 @@ mgr_status mgr_compute_level_populations(mgr_handle *h, const mgr_ali_opts *opts
         bool more = true;
         while (more && iteration < opts->max_iter) {
             iteration++;
-            if (opts->use_ng && normal == 4) {
+            if (opts->use_ng && normal == ng_every) {
                 h->launches += graph ? graph_run(h, h->g_ng, 0, [&] { return enqueue_ng(h); })
                                      : enqueue_ng(h);
                 ck(cudaStreamSynchronize(h->stream), "ng");

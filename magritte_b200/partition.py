@@ -134,19 +134,24 @@ def all_gather_blocks(views, group=None):
 
 
 def partitioned_level_populations(shard, group=None, use_ng: bool = True, max_iter: int = 1000,
-                                  tol_max_rel: float = 0.0) -> Tuple[int, List[float], bool]:
+                                  tol_max_rel: float = 0.0,
+                                  ng_every: int = 0) -> Tuple[int, List[float], bool]:
     """The ALI loop of ``Simulation::compute_level_populations``
     (``src/Simulation/sim_lines.tpp:61-164``) over the shards of a process
-    group: Ng after every four normal iterations, stop at max relative
-    change < tol_max_rel (or, with tol_max_rel <= 0, the reference's
-    fraction_not_converged <= 0.005).  Returns (iterations, max relative
-    change of every iteration, converged); every rank returns the same."""
+    group: Ng after every ``ng_every`` normal iterations (0: the
+    reference's four), stop at max relative change < tol_max_rel (or, with
+    tol_max_rel <= 0, the reference's fraction_not_converged <= 0.005).
+    Returns (iterations, max relative change of every iteration,
+    converged); every rank returns the same."""
+    if ng_every != 0 and ng_every < 3:
+        raise ValueError("ng_every must be 0 (the reference's 4) or >= 3")
+    every = ng_every or 4
     iteration, normal = 0, 0
     hist: List[float] = []
     more = True
     while more and iteration < max_iter:
         iteration += 1
-        if use_ng and normal == 4:
+        if use_ng and normal == every:
             shard.ng_step()
             normal = 0
         else:

@@ -113,19 +113,22 @@ class Simulation:
 
     def compute_level_populations(self, use_Ng: bool = True, max_niterations: int = 1000,
                                   precision="fp64", tol_max_rel: float = 0.0,
-                                  use_graph: bool = False) -> int:
+                                  use_graph: bool = False, ng_every: int = 0) -> int:
         """ALI loop (``Simulation::compute_level_populations``,
         ``sim_lines.tpp:61-164``); returns the iteration count.
         ``tol_max_rel`` > 0 stops at max relative population change < tol;
-        ``use_graph`` replays each iteration's launches as CUDA graphs.  For
-        a batch of models every model iterates to its own convergence and
-        the count is the batch's (``segment_results`` has each model's)."""
+        ``use_graph`` replays each iteration's launches as CUDA graphs;
+        ``ng_every`` is the number of normal iterations before each Ng step
+        (0: the reference's 4; at least 3).  For a batch of models every
+        model iterates to its own convergence and the count is the batch's
+        (``segment_results`` has each model's)."""
         o = _capi.AliOpts()
         o.use_ng = int(bool(use_Ng))
         o.precision = _PREC[precision]
         o.max_iter = int(max_niterations)
         o.tol_max_rel = float(tol_max_rel)
         o.use_graph = int(bool(use_graph))
+        o.ng_every = int(ng_every)
         it = C.c_int64(0)
         hist = np.zeros(max(1, int(max_niterations)))
         st = self._ck(self._lib.mgr_compute_level_populations(self._h, C.byref(o), C.byref(it),

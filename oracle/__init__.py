@@ -97,6 +97,9 @@ def lib():
         L.orc_raypair_lambda_row.argtypes = [_i64, _i64, _P, _P, _i64, _P, _P, _P]
         L.orc_compute_level_populations.restype = _i64
         L.orc_compute_level_populations.argtypes = [_P, _P, _P, C.c_int, _i64, _dbl, C.c_int, _P]
+        L.orc_compute_level_populations_ng.restype = _i64
+        L.orc_compute_level_populations_ng.argtypes = [_P, _P, _P, C.c_int, _i64, _dbl, C.c_int,
+                                                       _P, C.c_int]
         _lib = L
     return _lib
 
@@ -379,10 +382,12 @@ class Oracle:
         lib().orc_set_emissivity_opacity(self.M, self.S)
 
     def compute_level_populations(self, use_ng: bool = True, max_iter: int = 1000,
-                                  tol_max_rel: float = 0.0, nthreads: int = 0):
+                                  tol_max_rel: float = 0.0, nthreads: int = 0,
+                                  ng_every: int = 4):
         hist = np.zeros(max_iter)
-        it = lib().orc_compute_level_populations(self.M, self.S, _ptr(self.antipod), int(use_ng),
-                                                 max_iter, tol_max_rel, nthreads, _ptr(hist))
+        it = lib().orc_compute_level_populations_ng(self.M, self.S, _ptr(self.antipod),
+                                                    int(use_ng), max_iter, tol_max_rel, nthreads,
+                                                    _ptr(hist), int(ng_every))
         return int(it), hist[:it].copy()
 
     @property

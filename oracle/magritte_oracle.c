@@ -1516,17 +1516,19 @@ void orc_ng_acceleration(const orc_model *m, orc_state *s)
 
 /* Simulation::compute_level_populations(io, use_Ng, max_niterations),
  * Simulation/sim_lines.tpp:61-164.  tol_max_rel > 0 replaces the stop test
- * "fraction_not_converged <= 0.005" by "max relative change < tol_max_rel". */
-int64_t orc_compute_level_populations(const orc_model *m, orc_state *s, const int64_t *antipod,
-                                      int use_ng, int64_t max_iter, double tol_max_rel,
-                                      int nthreads, double *iter_max_rel)
+ * "fraction_not_converged <= 0.005" by "max relative change < tol_max_rel".
+ * ng_every: normal iterations before each Ng step (the reference: 4). */
+int64_t orc_compute_level_populations_ng(const orc_model *m, orc_state *s,
+                                         const int64_t *antipod, int use_ng, int64_t max_iter,
+                                         double tol_max_rel, int nthreads, double *iter_max_rel,
+                                         int ng_every)
 {
     int64_t iteration = 0, iteration_normal = 0;
     int some_not_converged = 1;
     while (some_not_converged && iteration < max_iter) {
         iteration++;
         some_not_converged = 0;
-        if (use_ng && iteration_normal == 4) {
+        if (use_ng && iteration_normal == ng_every) {
             orc_ng_acceleration(m, s);
             orc_check_convergence(m, s);
             orc_set_emissivity_opacity(m, s);
@@ -1544,4 +1546,12 @@ int64_t orc_compute_level_populations(const orc_model *m, orc_state *s, const in
         else if (s->fnc > 0.005) some_not_converged = 1;
     }
     return iteration;
+}
+
+int64_t orc_compute_level_populations(const orc_model *m, orc_state *s, const int64_t *antipod,
+                                      int use_ng, int64_t max_iter, double tol_max_rel,
+                                      int nthreads, double *iter_max_rel)
+{
+    return orc_compute_level_populations_ng(m, s, antipod, use_ng, max_iter, tol_max_rel,
+                                            nthreads, iter_max_rel, 4);
 }

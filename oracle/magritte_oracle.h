@@ -161,6 +161,11 @@ void orc_ng_acceleration(const orc_model *m, orc_state *s);
 int64_t orc_compute_level_populations(const orc_model *m, orc_state *s, const int64_t *antipod,
                                       int use_ng, int64_t max_iter, double tol_max_rel,
                                       int nthreads, double *iter_max_rel);
+/* The same with ng_every normal iterations before each Ng step. */
+int64_t orc_compute_level_populations_ng(const orc_model *m, orc_state *s,
+                                         const int64_t *antipod, int use_ng, int64_t max_iter,
+                                         double tol_max_rel, int nthreads, double *iter_max_rel,
+                                         int ng_every);
 
 #ifdef __cplusplus
 }

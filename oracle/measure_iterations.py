@@ -24,13 +24,14 @@ sys.path.insert(0, ROOT)
 TOL = 1.0e-4
 
 
-def step_kinds(iterations: int, use_ng: bool = True):
+def step_kinds(iterations: int, use_ng: bool = True, ng_every: int = 4):
     """Kinds of the iterations of the reference's loop: 'solve' (formal
     solve + Jeff + statistical equilibrium) or 'ng' (sim_lines.tpp:110-118:
-    an Ng step after every four normal iterations, counted as an iteration)."""
+    an Ng step after every four normal iterations, counted as an
+    iteration; ng_every normal iterations where the loop was run so)."""
     kinds, normal = [], 0
     for _ in range(iterations):
-        if use_ng and normal == 4:
+        if use_ng and normal == ng_every:
             kinds.append("ng")
             normal = 0
         else:

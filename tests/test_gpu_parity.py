@@ -116,13 +116,16 @@ def test_radiation_field_subset_config2_shape(gpu):
     assert rel_err(sim.Lambda[origins], orc.Ls[origins]) < FP64_RTOL
 
 
-def test_stateq_and_ng_iterations(gpu):
-    """Eight ALI iterations (one of them Ng) against the oracle."""
+@pytest.mark.parametrize("ng_every", [0, 3])
+def test_stateq_and_ng_iterations(gpu, ng_every):
+    """Eight ALI iterations against the oracle: Ng at the 5th (the
+    reference's cadence) or at the 4th and 8th (ng_every = 3)."""
     model = small_wind(10, 5, 7)
     sim, orc = setup_pair(model, keep_J=False)
     it_gpu = sim.compute_level_populations(use_Ng=True, max_niterations=8, precision="fp64",
-                                           tol_max_rel=1e-30)
-    it_cpu, hist = orc.compute_level_populations(use_ng=True, max_iter=8, tol_max_rel=1e-30)
+                                           tol_max_rel=1e-30, ng_every=ng_every)
+    it_cpu, hist = orc.compute_level_populations(use_ng=True, max_iter=8, tol_max_rel=1e-30,
+                                                 ng_every=ng_every or 4)
     assert it_gpu == it_cpu == 8
     pop_g = sim.population
     assert rel_err(pop_g, orc.pop, floor=1e-10 * model.population_tot.max()) < FP64_RTOL

@@ -404,6 +404,28 @@ def test_ng_matches_formula():
     assert np.array_equal(o.prev1.ravel(), P)
 
 
+def test_ng_cadence_keeps_the_fixed_point():
+    """ALI + Ng with three normal iterations before each Ng step (instead of
+    the reference's four): the Ng step falls on the 4th iteration, and the
+    iteration converges to the same populations."""
+    pops = {}
+    for ng in (4, 3):
+        orc = oracle.Oracle(M.config1()).setup()
+        it, hist = orc.compute_level_populations(True, 40, 1e-9, ng_every=ng)
+        assert hist[-1] < 1e-9
+        pops[ng] = orc.pop.copy()
+    p4, p3 = pops[4], pops[3]
+    mask = p4 > 1e-10 * p4.sum(1, keepdims=True)
+    assert np.max(np.abs(p3 - p4)[mask] / p4[mask]) < 1e-7
+    # the cadence itself: the first three iterations are the same normal
+    # ones; the 4th is the Ng step with ng_every = 3 and a normal one with 4
+    h = {}
+    for ng in (4, 3):
+        orc = oracle.Oracle(M.config1()).setup()
+        _, h[ng] = orc.compute_level_populations(True, 5, 1e-30, ng_every=ng)
+    assert np.array_equal(h[3][:3], h[4][:3]) and h[3][3] != h[4][3]
+
+
 def test_ali_oracle_converges_and_is_stationary():
     model = M.lattice_cloud(6, name="l6")
     o = oracle.Oracle(model).setup()
