@@ -691,6 +691,11 @@ void do_trace(mgr_handle *h) {
             logged = true;
         }
     }
+    if (!logged && h->hop_rays) {   // a log kept from an earlier trace is not used again
+        free_ptr((void *&)h->hop_cell);
+        free_ptr((void *&)h->hop_n);
+        h->hop_rays = 0;
+    }
     const HopLog hop_log{h->hop_cell, h->hop_n, (int)kHopCap};
     reset_flags(h);
     ck(launch_trace_count(h->mv, 0, N, h->len_all, h->flags, h->stream, logged ? &hop_log : nullptr),
