@@ -62,7 +62,7 @@ class OracleShard:
                 self.orc.relative_change_max)
 
 
-def _rank_main(rank, world, port, out):
+def _rank_main(rank, world, port, out, ng_every=0):
     import torch.distributed as dist
     os.environ["OMP_NUM_THREADS"] = "2"
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
@@ -70,7 +70,7 @@ def _rank_main(rank, world, port, out):
     try:
         shard = OracleShard(small_wind(), rank, world)
         it, hist, conv = P.partitioned_level_populations(shard, use_ng=True, max_iter=40,
-                                                         tol_max_rel=TOL)
+                                                         tol_max_rel=TOL, ng_every=ng_every)
         np.savez(f"{out}_{rank}.npz", it=it, hist=np.array(hist), conv=conv,
                  pop=shard.orc.pop)
     finally:
@@ -86,15 +86,18 @@ def _free_port():
     return port
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_partitioned_ali_reproduces_unpartitioned(world):
+@pytest.mark.parametrize("world,ng_every", [(2, 0), (3, 0), (2, 3)])
+def test_partitioned_ali_reproduces_unpartitioned(world, ng_every):
+    """ng_every = 3: the Ng step after three normal iterations, as the
+    oracle's ALI with the same option runs it."""
     import torch.multiprocessing as mp
     model = small_wind()
     ref = oracle.Oracle(model).setup()
-    it_ref, hist_ref = ref.compute_level_populations(True, 40, TOL, nthreads=2)
+    it_ref, hist_ref = ref.compute_level_populations(True, 40, TOL, nthreads=2,
+                                                     ng_every=ng_every or 4)
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "rank")
-        mp.start_processes(_rank_main, args=(world, _free_port(), out), nprocs=world,
+        mp.start_processes(_rank_main, args=(world, _free_port(), out, ng_every), nprocs=world,
                            join=True, start_method="spawn")
         res = [np.load(f"{out}_{r}.npz") for r in range(world)]
     for r in res:
