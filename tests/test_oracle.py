@@ -426,6 +426,17 @@ def test_ng_cadence_keeps_the_fixed_point():
     assert np.array_equal(h[3][:3], h[4][:3]) and h[3][3] != h[4][3]
 
 
+def test_step_kinds_follow_the_cadence():
+    """The iteration kinds the CPU baseline charges: an Ng step after every
+    four normal iterations (the reference), or after every three."""
+    from oracle.measure_iterations import step_kinds
+    assert step_kinds(5) == ["solve"] * 4 + ["ng"]
+    assert step_kinds(9) == (["solve"] * 4 + ["ng"]) + ["solve"] * 4
+    assert step_kinds(4, ng_every=3) == ["solve"] * 3 + ["ng"]
+    assert step_kinds(8, ng_every=3) == (["solve"] * 3 + ["ng"]) * 2
+    assert step_kinds(6, use_ng=False) == ["solve"] * 6
+
+
 def test_ali_oracle_converges_and_is_stationary():
     model = M.lattice_cloud(6, name="l6")
     o = oracle.Oracle(model).setup()
