@@ -5,9 +5,10 @@ linear rotor, 9 lines x 31 bins = 279 bins, 48 HEALPix rays = 24 pairs),
 seeded synthetic data.  One step is one complete solve of the hot path:
 trace every ray, set the starting populations (learned warm start by
 default, LTE with --start lte), and iterate formal solve + Jeff +
-statistical equilibrium (+ Ng every 5th iteration) until the max relative
-population change over all (cell, level) with n > 1e-10 n_tot drops below
-1e-4.  The headline arm is learned start + mixed precision; the plain FP64
+statistical equilibrium (+ an Ng step after every three normal iterations
+from the learned start, four -- the reference's cadence -- from LTE;
+--ng-every overrides) until the max relative population change over all
+(cell, level) with n > 1e-10 n_tot drops below 1e-4.  The headline arm is learned start + mixed precision; the plain FP64
 solve from LTE is measured in the same run and reported beside it.
 
     value  seconds per converged solve, device-timed (CUDA events on the
