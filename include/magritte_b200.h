@@ -95,7 +95,9 @@ typedef struct {
 } mgr_model_desc;
 
 /* Options of the ALI loop.  Replaces the arguments of
- * Simulation::compute_level_populations(io, use_Ng, max_niterations). */
+ * Simulation::compute_level_populations(io, use_Ng, max_niterations).
+ * A zeroed struct with use_ng, precision and max_iter set is the
+ * reference's loop. */
 typedef struct {
     int32_t use_ng;        /* Ng acceleration after every ng_every normal
                               iterations (the reference: every 5th
