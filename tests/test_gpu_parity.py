@@ -58,8 +58,13 @@ def setup_pair(model, keep_J=True):
 
 
 @pytest.mark.parametrize("make", [M.config1, lambda: small_wind(10, 5, 7),
-                                  lambda: M.wind_model(9, seed=3, nlev=4, nside=2, vmax=40e3)])
+                                  lambda: M.wind_model(9, seed=3, nlev=4, nside=2, vmax=40e3),
+                                  lambda: M.slab_1d(300, vmax=980.0)])
 def test_traces_bit_exact(gpu, make):
+    """Traced cells, shifts and increments equal the oracle's bit for bit.
+    The 300-cell slab has walks longer than the counting pass's hop log
+    holds (128 hops), which the fill searches again, beside shorter ones
+    that it replays."""
     model = make()
     sim = Simulation(model)
     orc = oracle.Oracle(model)
